@@ -1,0 +1,260 @@
+"""ctypes binding of libcintx_cuda.so (declarations in include/cintx_cuda.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcintx_cuda.so")
+
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+_vp = ctypes.c_void_p
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class CintxError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__("cintx status %d: %s" % (code, message))
+        self.code = code
+
+
+class PlanStats(ctypes.Structure):
+    _fields_ = [("nquartets", _i64), ("nintegrals", _i64), ("nchunks", _i64),
+                ("max_chunk_doubles", _i64), ("nprim_quartets", _i64), ("flops", _d)]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libcintx_cuda.so is not built (run python -m cintx_b200.build or "
+                          "__graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = [_dp, _ip, _ip, _ip, _i, _ip, _i, _dp, _vp, _dp]
+    for name in ("int2e_sph", "int2e_cart", "int3c2e_sph", "int3c2e_cart", "int2c2e_sph", "int2c2e_cart"):
+        f = getattr(L, name)
+        f.argtypes = sig
+        f.restype = _i
+    for name in ("int2e_optimizer", "int3c2e_optimizer", "int2c2e_optimizer"):
+        f = getattr(L, name)
+        f.argtypes = [ctypes.POINTER(_vp), _ip, _i, _ip, _i, _dp]
+        f.restype = None
+    L.CINTdel_optimizer.argtypes = [ctypes.POINTER(_vp)]
+    L.CINTdel_optimizer.restype = None
+    L.CINTrys_roots.argtypes = [_i, _d, _dp, _dp]
+    L.CINTrys_roots.restype = _i
+    L.cintx_rys_t2_batch.argtypes = [_i, _dp, _i64, _dp]
+    L.cintx_rys_t2_batch.restype = _i
+    L.cintx_cuda_last_error_code.restype = _i
+    L.cintx_cuda_last_error_message.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    L.cintx_cuda_last_error_message.restype = ctypes.c_size_t
+    L.cintx_cuda_clear_last_error.restype = None
+    L.cintx_plan_shells.argtypes = [ctypes.POINTER(_vp), _vp, _i, _ip, _i64, _i, _i64p]
+    L.cintx_plan_shells.restype = _i
+    L.cintx_plan_int2e_screened.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64]
+    L.cintx_plan_int2e_screened.restype = _i
+    L.cintx_plan_stats.argtypes = [_vp, ctypes.POINTER(PlanStats)]
+    L.cintx_plan_stats.restype = _i
+    L.cintx_plan_chunk_size.argtypes = [_vp, _i64]
+    L.cintx_plan_chunk_size.restype = _i64
+    L.cintx_plan_chunk_nquartets.argtypes = [_vp, _i64]
+    L.cintx_plan_chunk_nquartets.restype = _i64
+    L.cintx_plan_chunk_quartets.argtypes = [_vp, _i64, _ip, _i64]
+    L.cintx_plan_chunk_quartets.restype = _i
+    L.cintx_plan_execute.argtypes = [_vp, _i64, _vp, _vp]
+    L.cintx_plan_execute.restype = _i
+    L.cintx_plan_execute_host.argtypes = [_vp, _i64, _dp]
+    L.cintx_plan_execute_host.restype = _i
+    L.cintx_plan_destroy.argtypes = [_vp]
+    L.cintx_plan_destroy.restype = None
+    L.cintx_launch_count.restype = _i64
+    return L
+
+
+lib = _load()
+
+
+def last_error() -> tuple[int, str]:
+    buf = ctypes.create_string_buffer(1024)
+    lib.cintx_cuda_last_error_message(buf, 1024)
+    return lib.cintx_cuda_last_error_code(), buf.value.decode()
+
+
+def _check(code: int):
+    if code != 0:
+        c, m = last_error()
+        raise CintxError(code, m)
+
+
+def launch_count() -> int:
+    return int(lib.cintx_launch_count())
+
+
+def _arrs(atm, bas, env):
+    atm = np.ascontiguousarray(atm, dtype=np.int32)
+    bas = np.ascontiguousarray(bas, dtype=np.int32)
+    env = np.ascontiguousarray(env, dtype=np.float64)
+    return atm, bas, env
+
+
+def _block_len(bas, shls, sph):
+    n = 1
+    for s in shls:
+        l, nc = int(bas[s, 1]), int(bas[s, 3])
+        n *= (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
+    return n
+
+
+def _call(name, nsh, shls, atm, bas, env, opt=None, dims=None, out=None, sph=True):
+    atm, bas, env = _arrs(atm, bas, env)
+    s = np.ascontiguousarray(shls, dtype=np.int32)
+    assert s.size == nsh
+    if out is None:
+        n = _block_len(bas, s, sph) if dims is None else int(np.prod(dims))
+        out = np.zeros(n)
+    d = None if dims is None else np.ascontiguousarray(dims, dtype=np.int32)
+    ret = getattr(lib, name)(out.ctypes.data_as(_dp), None if d is None else d.ctypes.data_as(_ip),
+                             s.ctypes.data_as(_ip), atm.ctypes.data_as(_ip), atm.shape[0],
+                             bas.ctypes.data_as(_ip), bas.shape[0], env.ctypes.data_as(_dp),
+                             None if opt is None else opt.handle, None)
+    code = lib.cintx_cuda_last_error_code()
+    if code:
+        raise CintxError(code, last_error()[1])
+    return out, ret
+
+
+def int2e_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int2e_sph", 4, shls, atm, bas, env, opt, dims, out, True)
+
+
+def int2e_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int2e_cart", 4, shls, atm, bas, env, opt, dims, out, False)
+
+
+def int3c2e_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int3c2e_sph", 3, shls, atm, bas, env, opt, dims, out, True)
+
+
+def int3c2e_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int3c2e_cart", 3, shls, atm, bas, env, opt, dims, out, False)
+
+
+def int2c2e_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int2c2e_sph", 2, shls, atm, bas, env, opt, dims, out, True)
+
+
+def int2c2e_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int2c2e_cart", 2, shls, atm, bas, env, opt, dims, out, False)
+
+
+def rys_roots(n: int, x: float):
+    """libcint CINTrys_roots convention: u = t^2/(1-t^2) and weights."""
+    u = np.zeros(n)
+    w = np.zeros(n)
+    _check(lib.CINTrys_roots(n, float(x), u.ctypes.data_as(_dp), w.ctypes.data_as(_dp)))
+    return u, w
+
+
+def rys_t2_batch(n: int, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros((x.size, 2 * n))
+    _check(lib.cintx_rys_t2_batch(n, x.ctypes.data_as(_dp), x.size, out.ctypes.data_as(_dp)))
+    return out[:, :n], out[:, n:]
+
+
+class Optimizer:
+    """Owns a CINTOpt handle (device-resident basis and primitive-pair tables)."""
+
+    _makers = {0: "int2e_optimizer", 1: "int3c2e_optimizer", 2: "int2c2e_optimizer"}
+
+    def __init__(self, atm, bas, env, family: int = 0):
+        self.atm, self.bas, self.env = _arrs(atm, bas, env)
+        self.handle = _vp()
+        getattr(lib, self._makers[family])(ctypes.byref(self.handle), self.atm.ctypes.data_as(_ip),
+                                           self.atm.shape[0], self.bas.ctypes.data_as(_ip),
+                                           self.bas.shape[0], self.env.ctypes.data_as(_dp))
+        if not self.handle:
+            raise CintxError(*last_error())
+
+    def close(self):
+        if self.handle:
+            lib.CINTdel_optimizer(ctypes.byref(self.handle))
+            self.handle = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """A batched device evaluation plan (cintx_plan_* in include/cintx_cuda.h)."""
+
+    def __init__(self, handle, opt: Optimizer, offsets=None):
+        self.handle = handle
+        self.opt = opt  # keeps the optimizer alive
+        self.offsets = offsets
+
+    @classmethod
+    def shells(cls, opt: Optimizer, family: int, tuples, sph: bool = True):
+        t = np.ascontiguousarray(tuples, dtype=np.int32)
+        nsh = 4 if family == 0 else (3 if family == 1 else 2)
+        t = t.reshape(-1, nsh)
+        offs = np.zeros(t.shape[0], dtype=np.int64)
+        h = _vp()
+        _check(lib.cintx_plan_shells(ctypes.byref(h), opt.handle, family, t.ctypes.data_as(_ip), t.shape[0],
+                                     int(sph), offs.ctypes.data_as(_i64p)))
+        return cls(h, opt, offs)
+
+    @classmethod
+    def screened(cls, opt: Optimizer, cutoff: float = 1e-12, sph: bool = True, max_chunk_doubles: int = 1 << 28):
+        h = _vp()
+        _check(lib.cintx_plan_int2e_screened(ctypes.byref(h), opt.handle, float(cutoff), int(sph),
+                                             int(max_chunk_doubles)))
+        return cls(h, opt)
+
+    @property
+    def stats(self) -> PlanStats:
+        s = PlanStats()
+        _check(lib.cintx_plan_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def chunk_size(self, chunk: int) -> int:
+        return int(lib.cintx_plan_chunk_size(self.handle, chunk))
+
+    def chunk_quartets(self, chunk: int) -> np.ndarray:
+        n = int(lib.cintx_plan_chunk_nquartets(self.handle, chunk))
+        q = np.zeros((max(n, 0), 4), dtype=np.int32)
+        _check(lib.cintx_plan_chunk_quartets(self.handle, chunk, q.ctypes.data_as(_ip), n))
+        return q
+
+    def execute(self, out_ptr: int, chunk: int = -1, stream: int = 0):
+        """Asynchronous device execution into device pointer out_ptr."""
+        _check(lib.cintx_plan_execute(self.handle, chunk, ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)))
+
+    def execute_host(self, out: np.ndarray, chunk: int = -1):
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        _check(lib.cintx_plan_execute_host(self.handle, chunk, out.ctypes.data_as(_dp)))
+        return out
+
+    def close(self):
+        if self.handle:
+            lib.cintx_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

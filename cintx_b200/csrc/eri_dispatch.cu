@@ -1,0 +1,24 @@
+// Class dispatch entry used by the host code (kept in a CUDA translation unit).
+#include "eri_launch.cuh"
+#include "host_internal.h"
+
+namespace cintx {
+
+cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
+                         const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
+                         double expcutoff, const RysTable& rys, cudaStream_t stream) {
+  LaunchArgs a;
+  a.recs = recs;
+  a.nrec = nrec;
+  a.pairs = pairs;
+  a.prims = prims;
+  a.out = out;
+  a.st = st;
+  a.expcutoff = expcutoff;
+  a.rys = rys;
+  a.stream = stream;
+  a.max_blocks = 0;
+  return dispatch_eri(li, lj, lk, ll, sph, a);
+}
+
+}  // namespace cintx

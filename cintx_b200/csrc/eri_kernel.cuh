@@ -1,0 +1,486 @@
+// Fused Rys-quadrature ERI kernel for one angular-momentum class (LI LJ | LK LL).
+//
+// Work unit: one contracted shell quartet (ij|kl), processed by a group of S threads
+// (S = 1 .. 256, a power of two).  Per surviving primitive quartet the group computes
+//   1. x = a0 |P-Q|^2 and the prefactor (CINTg0_2e, g2e.c:4425-4475),
+//   2. the NR Rys roots/weights (rys_roots.cuh; lanes split the 2*NR table polynomials),
+//   3. the 3*NR (axis, root) 2D recurrences (VRR, CINTg0_2e_2d g2e.c:272) built on centres
+//      i and k, each followed by the horizontal transfer to j and l (g2e.c:428-694) in closed
+//      binomial form I(i,j) = sum_a C(j,a) (A-B)^(j-a) G(i+a), from registers into shared memory,
+//   4. the cartesian products sum_r Ix Iy Iz (CINTgout2e, cint2e.c:961) accumulated in
+//      registers: each lane owns whole (fj,fk,fl) tuples and all fi of each tuple.
+// After the primitive loop the i-axis cart->sph transform (c2s_sph_2e1, cart2sph.c:5324) is
+// applied in registers, the j/k axes in shared memory, and the l axis on the way to global
+// memory, with consecutive lanes writing consecutive doubles of the libcint-layout block.
+//
+// Shell pairs are oriented so that LI >= LJ and LK >= LL (the VRR is built on the larger
+// angular momentum, libcint's ibase/kbase choice, g2e.c:98-116).  Output strides let a launch
+// write any requested index order of the block.
+#pragma once
+#include "common.h"
+#include "c2s_coef.h"
+#include "rys_roots.cuh"
+
+namespace cintx {
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int cart_x(int l, int f) {
+  int lx = l;
+  while (f >= l - lx + 1) { f -= l - lx + 1; --lx; }
+  return lx;
+}
+__host__ __device__ constexpr int cart_y(int l, int f) {
+  int lx = l;
+  while (f >= l - lx + 1) { f -= l - lx + 1; --lx; }
+  return l - lx - f;
+}
+__host__ __device__ constexpr int cart_z(int l, int f) { return l - cart_x(l, f) - cart_y(l, f); }
+__host__ __device__ constexpr int binom(int n, int k) {
+  int r = 1;
+  for (int i = 0; i < k; ++i) r = r * (n - i) / (i + 1);
+  return r;
+}
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Threads per quartet: smallest power of two keeping <= 24 accumulators per lane, capped by
+// the tuple count and by 256.
+__host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll) {
+  const int ntup = ncart(lj) * ncart(lk) * ncart(ll);
+  const int total = ntup * ncart(li);
+  int s = 1;
+  while (s < 256 && (total + s - 1) / s > 24 && s * 2 <= ntup * 2) s *= 2;
+  return s;
+}
+
+template <int LI, int LJ, int LK, int LL, bool SPH>
+struct EriShape {
+  static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
+  static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
+  static constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
+  static constexpr int GSZ = NI * NJ * NK * NL;
+  static constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
+  static constexpr int NTUP = NFJ * NFK * NFL;
+  static constexpr int S = pick_threads(LI, LJ, LK, LL);
+  static constexpr int TPT = (NTUP + S - 1) / S;
+  static constexpr int MI = SPH && LI >= 2 ? 2 * LI + 1 : NFI;
+  static constexpr int MJ = SPH && LJ >= 2 ? 2 * LJ + 1 : NFJ;
+  static constexpr int MK = SPH && LK >= 2 ? 2 * LK + 1 : NFK;
+  static constexpr int ML = SPH && LL >= 2 ? 2 * LL + 1 : NFL;
+  static constexpr int NOUT = MI * MJ * MK * ML;
+  // shared memory per group (doubles): roots + g arrays during the primitive loop, two
+  // transform buffers afterwards (they alias)
+  static constexpr int SM_ROOTS = 2 * NR;
+  static constexpr int SM_G = 3 * NR * GSZ;
+  static constexpr int SM_BUFA = MI * NTUP;
+  static constexpr int SM_BUFB = MI * MJ * NFK * NFL;
+  static constexpr int NTASK_CONC = S < 3 * NR ? S : 3 * NR;  // tasks running at once
+  static constexpr int SM_SCR = NTASK_CONC * NIJ * NKL;          // per-task 2D tables
+  // classes whose transform buffers do not fit on chip keep them in a per-block global scratch
+  static constexpr bool GLOBAL_BUF = S > 1 && (SM_BUFA + SM_BUFB) * 8 * (S >= 128 ? 1 : 128 / S) > 200 * 1024;
+  static constexpr int GBUF_PER_BLOCK = GLOBAL_BUF ? SM_BUFA + SM_BUFB : 0;
+  static constexpr int SM_GROUP_RAW =
+      S == 1 ? 0 : cmax(SM_ROOTS + SM_G + SM_SCR, GLOBAL_BUF ? 0 : SM_BUFA + SM_BUFB);
+  static constexpr int SM_GROUP = (SM_GROUP_RAW + 1) & ~1;  // 16-byte multiple
+  static constexpr int BLOCK = S >= 128 ? S : 128;
+  static constexpr int Q = BLOCK / S;
+  static constexpr int SMEM_BYTES = Q * SM_GROUP * 8;
+};
+
+// Group barrier: warp-level for S <= 32, a named barrier per group above.
+template <int S>
+__device__ __forceinline__ void group_sync(int group) {
+  if constexpr (S == 1) {
+  } else if constexpr (S <= 32) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned base = lane & ~(unsigned)(S - 1);
+    const unsigned mask = (S == 32) ? 0xffffffffu : (((1u << S) - 1u) << base);
+    __syncwarp(mask);
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(S) : "memory");
+  }
+}
+
+// 2D recurrence for one (axis, root) followed by the horizontal transfers; writes
+// I[i + NI*(j + NJ*(k + NK*l))] to dst (stride 1).
+template <int LI, int LJ, int LK, int LL>
+__device__ __forceinline__ void vrr_hrr(double* __restrict__ dst, double g00, double c00, double c0p,
+                                        double b10, double b01, double b00, double ab, double cd) {
+  constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
+  constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
+  double G[NIJ][NKL];
+  G[0][0] = g00;
+#pragma unroll
+  for (int n = 1; n < NIJ; ++n)
+    G[n][0] = c00 * G[n - 1][0] + (n > 1 ? (n - 1) * b10 * G[n - 2][0] : 0.0);
+#pragma unroll
+  for (int m = 1; m < NKL; ++m) {
+#pragma unroll
+    for (int n = 0; n < NIJ; ++n) {
+      double v = c0p * G[n][m - 1];
+      if (m > 1) v += (m - 1) * b01 * G[n][m - 2];
+      if (n > 0) v += n * b00 * G[n - 1][m - 1];
+      G[n][m] = v;
+    }
+  }
+  double abp[LJ + 1], cdp[LL + 1];
+  abp[0] = 1.0;
+#pragma unroll
+  for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
+  cdp[0] = 1.0;
+#pragma unroll
+  for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
+#pragma unroll
+  for (int l = 0; l <= LL; ++l)
+#pragma unroll
+    for (int k = 0; k <= LK; ++k)
+#pragma unroll
+      for (int j = 0; j <= LJ; ++j)
+#pragma unroll
+        for (int i = 0; i <= LI; ++i) {
+          double v = 0.0;
+#pragma unroll
+          for (int a = 0; a <= j; ++a)
+#pragma unroll
+            for (int b = 0; b <= l; ++b)
+              v += (double)(binom(j, a) * binom(l, b)) * abp[j - a] * cdp[l - b] * G[i + a][k + b];
+          dst[i + NI * (j + NJ * (k + NK * l))] = v;
+        }
+}
+
+// Shared-memory version for the multi-lane path: the 2D table lives in gs[n*NKL + m]; the
+// horizontal transfers are unrolled over j and the (k, l) outputs, looped over i.
+template <int LI, int LJ, int LK, int LL>
+__device__ __forceinline__ void vrr_hrr_smem(double* __restrict__ dst, double* __restrict__ gs, double g00,
+                                             double c00, double c0p, double b10, double b01, double b00,
+                                             double ab, double cd) {
+  constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
+  constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
+  {
+    double gm2 = 0.0, gm1 = g00;
+    gs[0] = g00;
+    for (int n = 1; n < NIJ; ++n) {
+      const double g = c00 * gm1 + (n - 1) * b10 * gm2;
+      gs[n * NKL] = g;
+      gm2 = gm1;
+      gm1 = g;
+    }
+  }
+  for (int m = 1; m < NKL; ++m) {
+    for (int n = 0; n < NIJ; ++n) {
+      double v = c0p * gs[n * NKL + m - 1];
+      if (m > 1) v += (m - 1) * b01 * gs[n * NKL + m - 2];
+      if (n > 0) v += n * b00 * gs[(n - 1) * NKL + m - 1];
+      gs[n * NKL + m] = v;
+    }
+  }
+  double abp[LJ + 1], cdp[LL + 1];
+  abp[0] = 1.0;
+#pragma unroll
+  for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
+  cdp[0] = 1.0;
+#pragma unroll
+  for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
+  for (int i = 0; i <= LI; ++i) {
+#pragma unroll
+    for (int j = 0; j <= LJ; ++j) {
+      double T[NKL];
+#pragma unroll
+      for (int m = 0; m < NKL; ++m) {
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a <= j; ++a) v += (double)binom(j, a) * abp[j - a] * gs[(i + a) * NKL + m];
+        T[m] = v;
+      }
+#pragma unroll
+      for (int l = 0; l <= LL; ++l)
+#pragma unroll
+        for (int k = 0; k <= LK; ++k) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b <= l; ++b) v += (double)binom(l, b) * cdp[l - b] * T[k + b];
+          dst[i + NI * (j + NJ * (k + NK * l))] = v;
+        }
+    }
+  }
+}
+
+// Per-lane handles on the tuples it owns.
+template <class SH>
+struct LaneTuples {
+  int ox[SH::TPT], oy[SH::TPT], oz[SH::TPT];
+};
+
+template <class SH, int LJ, int LK, int LL>
+__device__ __forceinline__ void decode_tuples(LaneTuples<SH>& lt, int lane) {
+#pragma unroll
+  for (int k = 0; k < SH::TPT; ++k) {
+    int t = lane + SH::S * k;
+    if (t >= SH::NTUP) t = 0;
+    const int fj = t % SH::NFJ;
+    const int fk = (t / SH::NFJ) % SH::NFK;
+    const int fl = t / (SH::NFJ * SH::NFK);
+    int jx = 0, jy = 0, kx = 0, ky = 0, lx = 0, ly = 0;
+    // runtime cartesian decomposition (tiny loops; done once per kernel)
+    {
+      int f = fj, x = LJ;
+      while (f >= LJ - x + 1) { f -= LJ - x + 1; --x; }
+      jx = x; jy = LJ - x - f;
+    }
+    {
+      int f = fk, x = LK;
+      while (f >= LK - x + 1) { f -= LK - x + 1; --x; }
+      kx = x; ky = LK - x - f;
+    }
+    {
+      int f = fl, x = LL;
+      while (f >= LL - x + 1) { f -= LL - x + 1; --x; }
+      lx = x; ly = LL - x - f;
+    }
+    const int jz = LJ - jx - jy, kz = LK - kx - ky, lz = LL - lx - ly;
+    constexpr int SJ = SH::NI, SK = SH::NI * SH::NJ, SL = SH::NI * SH::NJ * SH::NK;
+    lt.ox[k] = jx * SJ + kx * SK + lx * SL;
+    lt.oy[k] = jy * SJ + ky * SK + ly * SL;
+    lt.oz[k] = jz * SJ + kz * SK + lz * SL;
+  }
+}
+
+template <int LI, int LJ, int LK, int LL, bool SPH>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK)
+    eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
+                 const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
+                 double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch) {
+  using SH = EriShape<LI, LJ, LK, LL, SPH>;
+  constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
+  extern __shared__ __align__(16) double smem[];
+  const int group = threadIdx.x / S;
+  const int lane = threadIdx.x % S;
+  double* sg = smem + group * SH::SM_GROUP;
+  double* s_roots = sg;                 // t2[NR], w[NR]
+  double* s_g = sg + SH::SM_ROOTS;      // [axis][root][GSZ]
+  double* s_scr = s_g + SH::SM_G;       // per-lane 2D tables (lanes < 3*NR)
+
+  LaneTuples<SH> lt;
+  decode_tuples<SH, LJ, LK, LL>(lt, lane);
+
+  // per-thread register storage used when S == 1
+  double r_roots[S == 1 ? 2 * NR : 1];
+  double r_g[S == 1 ? 3 * NR * GSZ : 1];
+
+  for (int q = blockIdx.x * SH::Q + group; q < nrec; q += gridDim.x * SH::Q) {
+    const QuartetRec rec = recs[q];
+    const ShellPair pij = pairs[rec.pij];
+    const ShellPair pkl = pairs[rec.pkl];
+    double acc[TPT][NFI];
+#pragma unroll
+    for (int k = 0; k < TPT; ++k)
+#pragma unroll
+      for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
+
+    for (int b = 0; b < pkl.nprim; ++b) {
+      const PrimPair pk = prims[pkl.prim_off + b];
+      const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+      for (int a = 0; a < pij.nprim; ++a) {
+        const PrimPair pi = prims[pij.prim_off + a];
+        if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
+        const double aij = pi.aij, akl = pk.aij;
+        const double aijkl = aij + akl;
+        const double rs = rsqrt(aijkl);
+        const double inv_aijkl = rs * rs;
+        const double a1 = aij * akl;
+        const double inv_a1 = 4.0 * pi.half_inv * pk.half_inv;
+        const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
+        const double rr = pqx * pqx + pqy * pqy + pqz * pqz;
+        const double x = a1 * inv_aijkl * rr;
+        const double fac = pi.kab * pk.kab * rs * inv_a1;
+        const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
+
+        double* groots;
+        double* gg;
+        if constexpr (S == 1) {
+          rys_all<NR>(rys, x, r_roots, r_roots + NR);
+          groots = r_roots;
+          gg = r_g;
+        } else {
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+          group_sync<S>(group);
+          groots = s_roots;
+          gg = s_g;
+        }
+        // (axis, root) recurrences
+        if constexpr (S == 1) {
+#pragma unroll
+          for (int task = 0; task < 3 * NR; ++task) {
+            const int axis = task / NR, r = task % NR;
+            const double t2 = groots[r];
+            const double rt_aa = t2 * inv_aijkl;
+            const double b00 = 0.5 * rt_aa;
+            const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
+            const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
+            const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
+            const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
+            const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
+            const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
+            const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
+            const double g00 = axis == 2 ? groots[NR + r] * fac : 1.0;
+            vrr_hrr<LI, LJ, LK, LL>(gg + task * GSZ, g00, pa - rt_aa * akl * pq, qc + rt_aa * aij * pq,
+                                    b10, b01, b00, ab, cd);
+          }
+        } else {
+          for (int task = lane; task < 3 * NR; task += S) {
+            const int axis = task / NR, r = task % NR;
+            const double t2 = groots[r];
+            const double rt_aa = t2 * inv_aijkl;
+            const double b00 = 0.5 * rt_aa;
+            const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
+            const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
+            const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
+            const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
+            const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
+            const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
+            const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
+            const double g00 = axis == 2 ? groots[NR + r] * fac : 1.0;
+            vrr_hrr_smem<LI, LJ, LK, LL>(gg + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), g00,
+                                         pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01, b00, ab, cd);
+          }
+          group_sync<S>(group);
+        }
+        // cartesian products, summed over roots
+#pragma unroll(SH::NR * SH::TPT * SH::NFI <= 256 ? SH::NR : 1)
+        for (int r = 0; r < NR; ++r) {
+          const double* gx = gg + (0 * NR + r) * GSZ;
+          const double* gy = gg + (1 * NR + r) * GSZ;
+          const double* gz = gg + (2 * NR + r) * GSZ;
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+            for (int fi = 0; fi < NFI; ++fi) {
+              acc[k][fi] = fma(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
+                               gz[cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
+            }
+          }
+        }
+        if constexpr (S > 1) group_sync<S>(group);
+      }
+    }
+
+    // ---- transform to spherical and store ----
+    double* const obase = out + rec.out;
+    if constexpr (S == 1) {
+      // whole block in registers: TPT == NTUP
+#pragma unroll
+      for (int ml = 0; ml < SH::ML; ++ml)
+#pragma unroll
+        for (int mk = 0; mk < SH::MK; ++mk)
+#pragma unroll
+          for (int mj = 0; mj < SH::MJ; ++mj)
+#pragma unroll
+            for (int mi = 0; mi < SH::MI; ++mi) {
+              double v = 0.0;
+#pragma unroll
+              for (int fl = 0; fl < SH::NFL; ++fl) {
+                constexpr bool sl = SPH && LL >= 2;
+                const double cl = sl ? c2s_coef(LL, ml, fl) : (ml == fl ? 1.0 : 0.0);
+                if (cl == 0.0) continue;
+#pragma unroll
+                for (int fk = 0; fk < SH::NFK; ++fk) {
+                  constexpr bool sk = SPH && LK >= 2;
+                  const double ck = sk ? c2s_coef(LK, mk, fk) : (mk == fk ? 1.0 : 0.0);
+                  if (ck == 0.0) continue;
+#pragma unroll
+                  for (int fj = 0; fj < SH::NFJ; ++fj) {
+                    constexpr bool sj = SPH && LJ >= 2;
+                    const double cj = sj ? c2s_coef(LJ, mj, fj) : (mj == fj ? 1.0 : 0.0);
+                    if (cj == 0.0) continue;
+#pragma unroll
+                    for (int fi = 0; fi < NFI; ++fi) {
+                      constexpr bool si = SPH && LI >= 2;
+                      const double ci = si ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+                      if (ci == 0.0) continue;
+                      v += ci * cj * ck * cl * acc[fj + SH::NFJ * (fk + SH::NFK * fl)][fi];
+                    }
+                  }
+                }
+              }
+              obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
+            }
+    } else {
+      double* bufA = SH::GLOBAL_BUF ? gscratch + (size_t)blockIdx.x * SH::GBUF_PER_BLOCK : sg;
+      double* bufB = bufA + SH::SM_BUFA;
+      // stage i in registers -> bufA[mi + MI * t], t = fj + NFJ*(fk + NFK*fl)
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) {
+        const int t = lane + S * k;
+        if (t < SH::NTUP) {
+#pragma unroll
+          for (int mi = 0; mi < SH::MI; ++mi) {
+            double v = 0.0;
+#pragma unroll
+            for (int fi = 0; fi < NFI; ++fi) {
+              const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+              if (c != 0.0) v += c * acc[k][fi];
+            }
+            bufA[mi + SH::MI * t] = v;
+          }
+        }
+      }
+      group_sync<S>(group);
+      // stage j: bufA[mi + MI*(fj + NFJ*(fk + NFK*fl))] -> bufB[mi + MI*(mj + MJ*(fk + NFK*fl))]
+      const double* cur = bufA;
+      if constexpr (SPH && LJ >= 2) {
+        constexpr int n = SH::MI * SH::MJ * SH::NFK * SH::NFL;
+        for (int o = lane; o < n; o += S) {
+          const int mi = o % SH::MI;
+          const int mj = (o / SH::MI) % SH::MJ;
+          const int rest = o / (SH::MI * SH::MJ);
+          const C2SRow& row = C2S_ROWS[LJ][mj];
+          double v = 0.0;
+          for (int z = 0; z < row.nnz; ++z) v += row.c[z] * bufA[mi + SH::MI * (row.f[z] + SH::NFJ * rest)];
+          bufB[o] = v;
+        }
+        group_sync<S>(group);
+        cur = bufB;
+      }
+      // stage k: cur[mi + MI*(mj + MJ*(fk + NFK*fl))] -> nxt[mi + MI*(mj + MJ*(mk + MK*fl))]
+      if constexpr (SPH && LK >= 2) {
+        double* nxt = (cur == bufA) ? bufB : bufA;
+        constexpr int n = SH::MI * SH::MJ * SH::MK * SH::NFL;
+        for (int o = lane; o < n; o += S) {
+          const int mij = o % (SH::MI * SH::MJ);
+          const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
+          const int fl = o / (SH::MI * SH::MJ * SH::MK);
+          const C2SRow& row = C2S_ROWS[LK][mk];
+          double v = 0.0;
+          for (int z = 0; z < row.nnz; ++z)
+            v += row.c[z] * cur[mij + SH::MI * SH::MJ * (row.f[z] + SH::NFK * fl)];
+          nxt[o] = v;
+        }
+        group_sync<S>(group);
+        cur = nxt;
+      }
+      // stage l + store: cur[mijk + MIJK*fl] -> out
+      {
+        constexpr int n = SH::NOUT;
+        constexpr int MIJK = SH::MI * SH::MJ * SH::MK;
+        for (int o = lane; o < n; o += S) {
+          const int mi = o % SH::MI;
+          const int mj = (o / SH::MI) % SH::MJ;
+          const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
+          const int ml = o / MIJK;
+          const int mijk = o % MIJK;
+          double v;
+          if constexpr (SPH && LL >= 2) {
+            const C2SRow& row = C2S_ROWS[LL][ml];
+            v = 0.0;
+            for (int z = 0; z < row.nnz; ++z) v += row.c[z] * cur[mijk + MIJK * row.f[z]];
+          } else {
+            v = cur[mijk + MIJK * ml];
+          }
+          obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
+        }
+      }
+      group_sync<S>(group);
+    }
+  }
+}
+
+}  // namespace cintx

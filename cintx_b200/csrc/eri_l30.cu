@@ -1,0 +1,7 @@
+// Kernels and dispatch for classes whose first shell pair has angular momenta (3, 0).
+#include "eri_launch.cuh"
+namespace cintx {
+cudaError_t dispatch_l30(int lk, int ll, bool sph, const LaunchArgs& a) {
+  return dispatch_lij<3, 0>(lk, ll, sph, a);
+}
+}  // namespace cintx

@@ -1,0 +1,117 @@
+// Launch helpers for the per-class ERI kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <type_traits>
+#include "eri_kernel.cuh"
+
+namespace cintx {
+
+struct LaunchArgs {
+  const QuartetRec* recs;
+  int nrec;
+  const ShellPair* pairs;
+  const PrimPair* prims;
+  double* out;
+  OutStrides st;
+  double expcutoff;
+  RysTable rys;
+  cudaStream_t stream;
+  int max_blocks;  // grid cap (0: derived from the SM count)
+};
+
+// Device scratch for classes whose transform buffers live in global memory: returns a buffer
+// of at least `bytes` owned by the calling host thread (ordered by that thread's launches).
+double* class_scratch(size_t bytes);
+
+// A class is compiled when both pairs are oriented (la >= lb) and the first pair is not
+// lower than the second in (la, lb) order.
+__host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
+  return li >= lj && lk >= ll && (li > lk || (li == lk && lj >= ll));
+}
+
+int device_sm_count();
+
+template <int LI, int LJ, int LK, int LL, bool SPH>
+cudaError_t launch_eri(const LaunchArgs& a) {
+  using SH = EriShape<LI, LJ, LK, LL, SPH>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH>;
+  static int attr_done[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (SH::SMEM_BYTES > 48 * 1024 && dev < 64 && !attr_done[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr_done[dev] = 1;
+  }
+  if (a.nrec <= 0) return cudaSuccess;
+  long long blocks = ((long long)a.nrec + SH::Q - 1) / SH::Q;
+  long long cap = a.max_blocks > 0 ? a.max_blocks : (long long)device_sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  double* scratch = nullptr;
+  if constexpr (SH::GLOBAL_BUF) {
+    if (blocks > 2LL * device_sm_count()) blocks = 2LL * device_sm_count();
+    scratch = class_scratch(sizeof(double) * (size_t)SH::GBUF_PER_BLOCK * (size_t)blocks);
+    if (!scratch) return cudaErrorMemoryAllocation;
+  }
+  kern<<<(unsigned)blocks, SH::BLOCK, SH::SMEM_BYTES, a.stream>>>(a.recs, a.nrec, a.pairs, a.prims, a.out,
+                                                                   a.st, a.expcutoff, a.rys, scratch);
+  return cudaGetLastError();
+}
+
+template <int N, class F>
+__host__ inline void static_for(F&& f) {
+  if constexpr (N > 0) {
+    static_for<N - 1>(f);
+    f(std::integral_constant<int, N - 1>{});
+  }
+}
+
+// Dispatch over (lk, ll) for a fixed (li, lj); cudaErrorInvalidValue for classes that are not
+// compiled.
+template <int LI, int LJ>
+cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
+  cudaError_t err = cudaErrorInvalidValue;
+  static_for<CINTX_LMAX + 1>([&](auto K) {
+    static_for<K.value + 1>([&](auto L) {
+      constexpr int k = decltype(K)::value, l = decltype(L)::value;
+      if constexpr (class_valid(LI, LJ, k, l)) {
+        if (lk == k && ll == l)
+          err = sph ? launch_eri<LI, LJ, k, l, true>(a) : launch_eri<LI, LJ, k, l, false>(a);
+      }
+    });
+  });
+  return err;
+}
+
+#define CINTX_DECL_DISPATCH(I, J) cudaError_t dispatch_l##I##J(int, int, bool, const LaunchArgs&);
+CINTX_DECL_DISPATCH(0, 0)
+CINTX_DECL_DISPATCH(1, 0) CINTX_DECL_DISPATCH(1, 1)
+CINTX_DECL_DISPATCH(2, 0) CINTX_DECL_DISPATCH(2, 1) CINTX_DECL_DISPATCH(2, 2)
+CINTX_DECL_DISPATCH(3, 0) CINTX_DECL_DISPATCH(3, 1) CINTX_DECL_DISPATCH(3, 2) CINTX_DECL_DISPATCH(3, 3)
+CINTX_DECL_DISPATCH(4, 0) CINTX_DECL_DISPATCH(4, 1) CINTX_DECL_DISPATCH(4, 2) CINTX_DECL_DISPATCH(4, 3)
+CINTX_DECL_DISPATCH(4, 4)
+#undef CINTX_DECL_DISPATCH
+
+inline cudaError_t dispatch_eri(int li, int lj, int lk, int ll, bool sph, const LaunchArgs& a) {
+  if (li > CINTX_LMAX || !class_valid(li, lj, lk, ll)) return cudaErrorInvalidValue;
+  switch (li * 10 + lj) {
+    case 0: return dispatch_l00(lk, ll, sph, a);
+    case 10: return dispatch_l10(lk, ll, sph, a);
+    case 11: return dispatch_l11(lk, ll, sph, a);
+    case 20: return dispatch_l20(lk, ll, sph, a);
+    case 21: return dispatch_l21(lk, ll, sph, a);
+    case 22: return dispatch_l22(lk, ll, sph, a);
+    case 30: return dispatch_l30(lk, ll, sph, a);
+    case 31: return dispatch_l31(lk, ll, sph, a);
+    case 32: return dispatch_l32(lk, ll, sph, a);
+    case 33: return dispatch_l33(lk, ll, sph, a);
+    case 40: return dispatch_l40(lk, ll, sph, a);
+    case 41: return dispatch_l41(lk, ll, sph, a);
+    case 42: return dispatch_l42(lk, ll, sph, a);
+    case 43: return dispatch_l43(lk, ll, sph, a);
+    case 44: return dispatch_l44(lk, ll, sph, a);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace cintx

@@ -1,0 +1,124 @@
+// Host-side internals shared by the C-ABI (host_api.cpp) and the planners (host_plan.cpp).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.h"
+
+struct CINTOpt;  // the library's optimizer handle (defined below as cintx::Opt)
+
+namespace cintx {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int ATM_SLOTS = 6, BAS_SLOTS = 8, PTR_COORD = 1;
+constexpr int ATOM_OF = 0, ANG_OF = 1, NPRIM_OF = 2, NCTR_OF = 3, PTR_EXP = 5, PTR_COEFF = 6;
+constexpr int PTR_EXPCUTOFF = 0, PTR_RANGE_OMEGA = 8;
+
+void set_error(int code, const std::string& msg);
+void clear_error();
+
+// One contracted shell of the caller's basis.
+struct ShellInfo {
+  int l, nprim, nctr, atom;
+  int vbase;  // first virtual shell (one per contraction)
+  double r[3];
+  std::vector<double> exps;
+  std::vector<double> coef;      // column-major [ctr][prim] as in env
+  std::vector<double> log_maxc;  // log max_ctr |c| per primitive (CINTOpt_log_max_pgto_coeff)
+};
+
+struct Basis {
+  int natm = 0, nbas = 0, nvirt = 0;
+  std::vector<int> atm, bas;
+  std::vector<double> env;
+  std::vector<ShellInfo> sh;
+  std::vector<int> vshell, vctr;  // virtual shell -> (shell, contraction)
+};
+
+// Validates and copies a libcint (atm, bas, env); env length is taken from the largest
+// pointer used.  Returns a status code.
+int load_basis(Basis& b, const int* atm, int natm, const int* bas, int nbas, const double* env);
+
+// Exponent cut-offs of libcint: int2e uses max(40, env[0]) + 1 (g2e.c:57-62), int3c2e and
+// int2c2e use max(40, env[0]) (g3c2e.c:55-59, g2c2e.c:46-50); 60 when env[0] == 0.
+double expcutoff_2e(const double* env);
+double expcutoff_3c(const double* env);
+
+// Host copy of an oriented shell pair (virtual shells a >= b in angular momentum; b < 0 is
+// the unit s function used for 3- and 2-centre integrals).
+struct PairHost {
+  int a = -1, b = -1;
+  int la = 0, lb = 0;
+  double min_cce = 1e300;
+  ShellPair sp{};
+  std::vector<PrimPair> prims;
+};
+
+// Builds the screened primitive pairs of virtual shells (a, b), in that order (b < 0: unit).
+void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out);
+
+// Device-resident state of one CINTOpt: all unordered virtual-shell pairs (u >= v) oriented by
+// angular momentum (larger l first; equal l keeps the larger index first) followed by one unit
+// pair per virtual shell.
+struct Opt {
+  uint64_t magic;
+  Basis basis;
+  double build_cutoff = 0;
+  int device = -1;
+  int npairs = 0;             // regular pairs; unit pair of v is npairs + v
+  std::vector<int> pair_a, pair_b, pair_la, pair_lb, pair_nprim;
+  std::vector<double> pair_min_cce;
+  ShellPair* d_pairs = nullptr;
+  PrimPair* d_prims = nullptr;
+  int64_t nprims_total = 0;
+  std::mutex mu;
+  static constexpr uint64_t kMagic = 0x43494e5458423230ull;  // "CINTXB20"
+};
+
+inline int pair_index(int u, int v) {  // unordered, u >= v
+  return u >= v ? u * (u + 1) / 2 + v : v * (v + 1) / 2 + u;
+}
+
+Opt* as_opt(CINTOpt* o);
+int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env);
+
+// Per-device constants (Rys table) and per-thread scratch.
+struct DeviceState {
+  int dev = -1;
+  void* rys_buf = nullptr;
+  RysTable rys{};
+};
+int device_state(DeviceState** out);  // for the current device
+
+struct ThreadScratch {
+  int dev = -1;
+  cudaStream_t stream = nullptr;
+  void* dbuf = nullptr;
+  size_t dcap = 0;
+  void* hbuf = nullptr;  // pinned
+  size_t hcap = 0;
+  int64_t launches = 0;
+};
+int thread_scratch(ThreadScratch** out, size_t dbytes, size_t hbytes);
+
+// Orientation of a requested shell tuple onto a compiled kernel class.
+struct Oriented {
+  int li, lj, lk, ll;       // kernel class
+  int src[4];               // requested axis feeding kernel axis c
+  bool swap_ab;             // kernel (ij) pair is the requested second pair
+};
+
+// Algorithmic FP64 flop count of the Rys path per primitive quartet and per contracted
+// quartet (c2s) for a class.
+double flops_per_prim_quartet(int li, int lj, int lk, int ll);
+double flops_c2s(int li, int lj, int lk, int ll, bool sph);
+
+cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
+                         const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
+                         double expcutoff, const RysTable& rys, cudaStream_t stream);
+
+}  // namespace cintx

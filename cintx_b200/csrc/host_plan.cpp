@@ -1,0 +1,652 @@
+// Batched plans: explicit shell-tuple lists and Schwarz-screened unique-quartet sweeps.
+//
+// A plan owns device work descriptions for one CINTOpt.  Its unit of execution is a chunk:
+// a list of segments, each one kernel class over a contiguous range of quartet records, with
+// the chunk's output blocks back to back (libcint layout per block).  Explicit plans keep
+// their records resident; screened plans regenerate each chunk's records on the device from
+// per-tile row prefixes (plan_kernels.cu), so no per-quartet host data exists for sweeps of
+// 1e10 quartets.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <numeric>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/cintx_cuda.h"
+#include "host_internal.h"
+
+namespace cintx {
+cudaError_t launch_gen_tile(const int* rows, const int* cols, const long long* row_prefix, int nrows,
+                            long long t0, long long t1, long long nout, long long out_base, QuartetRec* recs,
+                            cudaStream_t stream);
+}
+
+using namespace cintx;
+
+namespace {
+
+int nsph_or_cart(int l, bool sph) { return sph ? 2 * l + 1 : (l + 1) * (l + 2) / 2; }
+
+struct Segment {
+  int li, lj, lk, ll;
+  OutStrides st;
+  double expcutoff;
+  // explicit: records at d_recs[rec0, rec0+nrec); screened: tile index and quartet range
+  long long rec0 = 0;
+  long long nrec = 0;
+  int tile = -1;
+  long long t0 = 0, t1 = 0;
+  long long nout = 0;      // doubles per block (screened)
+  long long out_off = 0;   // chunk-relative output start of this segment
+};
+
+struct Chunk {
+  std::vector<Segment> segs;
+  long long out_size = 0;
+  long long nrec = 0;
+};
+
+struct Tile {
+  int typeA, typeB;
+  int li, lj, lk, ll;
+  std::vector<int> rows, cols;          // pair ids
+  std::vector<long long> row_prefix;    // size rows+1
+  int* d_rows = nullptr;
+  int* d_cols = nullptr;
+  long long* d_prefix = nullptr;
+};
+
+}  // namespace
+
+struct CintxPlan {
+  Opt* opt = nullptr;
+  int family = 0;
+  bool sph = true;
+  std::vector<Chunk> chunks;
+  std::vector<Tile> tiles;
+  QuartetRec* d_recs = nullptr;    // explicit: all records; screened: one chunk's records
+  long long rec_capacity = 0;
+  std::vector<QuartetRec> h_recs;  // explicit plans keep a host copy for chunk_quartets
+  std::vector<int> h_tuples;       // explicit: requested tuples (4 per record, -1 for unit)
+  CintxPlanStats stats{};
+  // end-to-end staging
+  double* d_stage = nullptr;
+  long long stage_cap = 0;
+  cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+void free_plan_device(CintxPlan* p) {
+  if (p->d_recs) cudaFree(p->d_recs);
+  p->d_recs = nullptr;
+  for (Tile& t : p->tiles) {
+    if (t.d_rows) cudaFree(t.d_rows);
+    if (t.d_cols) cudaFree(t.d_cols);
+    if (t.d_prefix) cudaFree(t.d_prefix);
+    t.d_rows = t.d_cols = nullptr;
+    t.d_prefix = nullptr;
+  }
+  if (p->d_stage) cudaFree(p->d_stage);
+  p->d_stage = nullptr;
+  if (p->stream) cudaStreamDestroy(p->stream);
+  p->stream = nullptr;
+}
+
+// Kernel class and strides for a quartet of oriented pairs (first pair is kernel (ij)).
+OutStrides canonical_strides(int li, int lj, int lk, bool sph) {
+  OutStrides st;
+  const long long n0 = nsph_or_cart(li, sph), n1 = nsph_or_cart(lj, sph), n2 = nsph_or_cart(lk, sph);
+  st.s0 = 1;
+  st.s1 = n0;
+  st.s2 = n0 * n1;
+  st.s3 = n0 * n1 * n2;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* shls, int64_t n, int sph,
+                      int64_t* offsets_out) {
+  clear_error();
+  if (!plan || !shls) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and shls must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  *plan = nullptr;
+  Opt* o = as_opt(optp);
+  if (!o) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "opt is not a handle created by this library");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  if (family < CINTX_INT2E || family > CINTX_INT2C2E || n < 0) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "unknown integral family");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (o->basis.env[PTR_RANGE_OMEGA] != 0.0) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "range-separated Coulomb is not supported");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  const Basis& B = o->basis;
+  const int nsh = family == CINTX_INT2E ? 4 : (family == CINTX_INT3C2E ? 3 : 2);
+  const double cutoff = family == CINTX_INT2E ? expcutoff_2e(B.env.data()) : expcutoff_3c(B.env.data());
+  CintxPlan* p = new CintxPlan();
+  p->opt = o;
+  p->family = family;
+  p->sph = sph != 0;
+  // group key -> records
+  struct GKey {
+    int li, lj, lk, ll;
+    long long s0, s1, s2, s3;
+    bool operator<(const GKey& o) const {
+      return std::tie(li, lj, lk, ll, s0, s1, s2, s3) < std::tie(o.li, o.lj, o.lk, o.ll, o.s0, o.s1, o.s2, o.s3);
+    }
+  };
+  std::map<GKey, std::vector<QuartetRec>> groups;
+  std::map<GKey, std::vector<int>> group_tuples;
+  long long off = 0;
+  double flops = 0;
+  long long nprimq = 0;
+  for (int64_t q = 0; q < n; ++q) {
+    const int* s = shls + q * nsh;
+    int rs[4];
+    bool unit[4] = {false, false, false, false};
+    if (family == CINTX_INT2E) {
+      for (int a = 0; a < 4; ++a) rs[a] = s[a];
+    } else if (family == CINTX_INT3C2E) {
+      rs[0] = s[0]; rs[1] = s[1]; rs[2] = s[2]; rs[3] = -1; unit[3] = true;
+    } else {
+      rs[0] = s[0]; rs[1] = -1; rs[2] = s[1]; rs[3] = -1; unit[1] = unit[3] = true;
+    }
+    int l[4], nc[4], ne[4];
+    for (int a = 0; a < 4; ++a) {
+      if (unit[a]) {
+        l[a] = 0; nc[a] = 1; ne[a] = 1;
+        continue;
+      }
+      if (rs[a] < 0 || rs[a] >= B.nbas) {
+        delete p;
+        set_error(CINTX_STATUS_INVALID_INPUT, "shell index out of range in tuple " + std::to_string(q));
+        return CINTX_STATUS_INVALID_INPUT;
+      }
+      l[a] = B.sh[rs[a]].l;
+      nc[a] = B.sh[rs[a]].nctr;
+      ne[a] = nsph_or_cart(l[a], p->sph);
+    }
+    long long counts[4], ast[4];
+    long long blk = 1;
+    for (int a = 0; a < 4; ++a) counts[a] = (long long)nc[a] * ne[a];
+    {
+      long long st = 1;
+      for (int a = 0; a < 4; ++a) {
+        ast[a] = unit[a] ? 0 : st;
+        if (!unit[a]) st *= counts[a];
+      }
+      blk = st;
+    }
+    if (offsets_out) offsets_out[q] = off;
+    for (int c3 = 0; c3 < nc[3]; ++c3)
+      for (int c2 = 0; c2 < nc[2]; ++c2)
+        for (int c1 = 0; c1 < nc[1]; ++c1)
+          for (int c0 = 0; c0 < nc[0]; ++c0) {
+            const int cs[4] = {c0, c1, c2, c3};
+            int v[4];
+            for (int a = 0; a < 4; ++a) v[a] = unit[a] ? -1 : B.sh[rs[a]].vbase + cs[a];
+            // pair ids with their table orientation
+            auto pair_of = [&](int x, int y, int& id, bool& x_first) {
+              if (y < 0) {
+                id = o->npairs + x;
+                x_first = true;
+              } else if (x < 0) {
+                id = o->npairs + y;
+                x_first = false;
+              } else {
+                id = pair_index(x, y);
+                x_first = (o->pair_a[id] == x);
+              }
+            };
+            int id1, id2;
+            bool f1, f2;
+            pair_of(v[0], v[1], id1, f1);
+            pair_of(v[2], v[3], id2, f2);
+            const int l1a = o->pair_la[id1], l1b = o->pair_lb[id1];
+            const int l2a = o->pair_la[id2], l2b = o->pair_lb[id2];
+            const bool swap = (l2a > l1a) || (l2a == l1a && l2b > l1b);
+            int src[4];
+            const int p1[2] = {f1 ? 0 : 1, f1 ? 1 : 0};
+            const int p2[2] = {f2 ? 2 : 3, f2 ? 3 : 2};
+            if (!swap) {
+              src[0] = p1[0]; src[1] = p1[1]; src[2] = p2[0]; src[3] = p2[1];
+            } else {
+              src[0] = p2[0]; src[1] = p2[1]; src[2] = p1[0]; src[3] = p1[1];
+            }
+            GKey k;
+            k.li = l[src[0]];
+            k.lj = l[src[1]];
+            k.lk = l[src[2]];
+            k.ll = l[src[3]];
+            k.s0 = ast[src[0]];
+            k.s1 = ast[src[1]];
+            k.s2 = ast[src[2]];
+            k.s3 = ast[src[3]];
+            QuartetRec r;
+            r.pij = swap ? id2 : id1;
+            r.pkl = swap ? id1 : id2;
+            long long o2 = off;
+            for (int a = 0; a < 4; ++a) o2 += (long long)cs[a] * ne[a] * ast[a];
+            r.out = o2;
+            groups[k].push_back(r);
+            for (int a = 0; a < 4; ++a) group_tuples[k].push_back(rs[a]);
+            const long long npq = (long long)o->pair_nprim[r.pij] * o->pair_nprim[r.pkl];
+            nprimq += npq;
+            flops += npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
+                     flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
+          }
+    off += blk;
+  }
+  Chunk ch;
+  long long rec0 = 0;
+  for (auto& kv : groups) {
+    Segment sg;
+    sg.li = kv.first.li;
+    sg.lj = kv.first.lj;
+    sg.lk = kv.first.lk;
+    sg.ll = kv.first.ll;
+    sg.st.s0 = kv.first.s0;
+    sg.st.s1 = kv.first.s1;
+    sg.st.s2 = kv.first.s2;
+    sg.st.s3 = kv.first.s3;
+    sg.expcutoff = cutoff;
+    sg.rec0 = rec0;
+    sg.nrec = (long long)kv.second.size();
+    sg.out_off = 0;
+    ch.segs.push_back(sg);
+    p->h_recs.insert(p->h_recs.end(), kv.second.begin(), kv.second.end());
+    auto& tu = group_tuples[kv.first];
+    p->h_tuples.insert(p->h_tuples.end(), tu.begin(), tu.end());
+    rec0 += sg.nrec;
+  }
+  ch.out_size = off;
+  ch.nrec = rec0;
+  p->chunks.push_back(ch);
+  p->rec_capacity = rec0;
+  if (rec0 > 0) {
+    if (cudaMalloc(&p->d_recs, sizeof(QuartetRec) * rec0) != cudaSuccess) {
+      delete p;
+      set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation of quartet records failed");
+      return CINTX_STATUS_ALLOCATION_FAILED;
+    }
+    cudaMemcpy(p->d_recs, p->h_recs.data(), sizeof(QuartetRec) * rec0, cudaMemcpyHostToDevice);
+  }
+  p->stats.nquartets = n;
+  p->stats.nintegrals = off;
+  p->stats.nchunks = 1;
+  p->stats.max_chunk_doubles = off;
+  p->stats.nprim_quartets = nprimq;
+  p->stats.flops = flops;
+  *plan = p;
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_execute(CintxPlan* p, int64_t chunk, double* out_dev, void* stream_) {
+  clear_error();
+  if (!p || !out_dev) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and out_dev must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (chunk >= (int64_t)p->chunks.size()) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "chunk index out of range");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  DeviceState* ds;
+  int rc;
+  if ((rc = device_state(&ds))) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!stream) {
+    ThreadScratch* ts;
+    if ((rc = thread_scratch(&ts, 0, 0))) return rc;
+    stream = ts->stream;
+  }
+  ThreadScratch* ts;
+  if ((rc = thread_scratch(&ts, 0, 0))) return rc;
+  const Opt* o = p->opt;
+  const int64_t c0 = chunk < 0 ? 0 : chunk, c1 = chunk < 0 ? (int64_t)p->chunks.size() : chunk + 1;
+  for (int64_t c = c0; c < c1; ++c) {
+    const Chunk& ch = p->chunks[c];
+    for (const Segment& sg : ch.segs) {
+      const QuartetRec* recs;
+      long long nrec;
+      if (sg.tile < 0) {
+        recs = p->d_recs + sg.rec0;
+        nrec = sg.nrec;
+      } else {
+        const Tile& t = p->tiles[sg.tile];
+        QuartetRec* dst = p->d_recs + sg.rec0;
+        cudaError_t e = launch_gen_tile(t.d_rows, t.d_cols, t.d_prefix, (int)t.rows.size(), sg.t0, sg.t1, sg.nout, 0,
+                                        dst, stream);
+        if (e != cudaSuccess) {
+          set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("quartet generation failed: ") + cudaGetErrorString(e));
+          return CINTX_STATUS_EXECUTION_FAILED;
+        }
+        ts->launches++;
+        recs = dst;
+        nrec = sg.t1 - sg.t0;
+      }
+      // the kernels take an int count; split very large segments
+      for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
+        const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
+        cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
+                                     out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream);
+        if (e != cudaSuccess) {
+          set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+          return CINTX_STATUS_EXECUTION_FAILED;
+        }
+        ts->launches++;
+      }
+    }
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_execute_host(CintxPlan* p, int64_t chunk, double* out_host) {
+  clear_error();
+  if (!p || !out_host) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and out_host must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (!p->stream && cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  const int64_t c0 = chunk < 0 ? 0 : chunk, c1 = chunk < 0 ? (int64_t)p->chunks.size() : chunk + 1;
+  long long need = 0;
+  for (int64_t c = c0; c < c1; ++c) need = std::max(need, p->chunks[c].out_size);
+  if (need > p->stage_cap) {
+    if (p->d_stage) cudaFree(p->d_stage);
+    if (cudaMalloc(&p->d_stage, sizeof(double) * std::max<long long>(need, 1)) != cudaSuccess) {
+      p->d_stage = nullptr;
+      p->stage_cap = 0;
+      set_error(CINTX_STATUS_ALLOCATION_FAILED, "device output staging allocation failed");
+      return CINTX_STATUS_ALLOCATION_FAILED;
+    }
+    p->stage_cap = need;
+  }
+  for (int64_t c = c0; c < c1; ++c) {
+    int rc = cintx_plan_execute(p, c, p->d_stage, p->stream);
+    if (rc) return rc;
+    cudaMemcpyAsync(out_host, p->d_stage, sizeof(double) * p->chunks[c].out_size, cudaMemcpyDeviceToHost, p->stream);
+  }
+  cudaError_t e = cudaStreamSynchronize(p->stream);
+  if (e != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("device execution failed: ") + cudaGetErrorString(e));
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_stats(const CintxPlan* p, CintxPlanStats* s) {
+  if (!p || !s) return CINTX_STATUS_NULL_POINTER;
+  *s = p->stats;
+  return CINTX_STATUS_SUCCESS;
+}
+
+int64_t cintx_plan_chunk_size(const CintxPlan* p, int64_t chunk) {
+  if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return -1;
+  return p->chunks[chunk].out_size;
+}
+
+int64_t cintx_plan_chunk_nquartets(const CintxPlan* p, int64_t chunk) {
+  if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return -1;
+  return p->chunks[chunk].nrec;
+}
+
+// Shell tuples of a chunk in output order (4 ints each; -1 for unit slots of 3c/2c plans).
+int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, int64_t cap) {
+  if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return CINTX_STATUS_INVALID_INPUT;
+  const Chunk& ch = p->chunks[chunk];
+  const Opt* o = p->opt;
+  int64_t k = 0;
+  for (const Segment& sg : ch.segs) {
+    if (sg.tile < 0) {
+      // explicit plans list tuples per record (group order), as requested
+      for (long long r = 0; r < sg.nrec; ++r, ++k) {
+        if (k >= cap) return CINTX_STATUS_BUFFER_TOO_SMALL;
+        for (int a = 0; a < 4; ++a) quartets[k * 4 + a] = p->h_tuples[(sg.rec0 + r) * 4 + a];
+      }
+    } else {
+      const Tile& t = p->tiles[sg.tile];
+      for (long long q = sg.t0; q < sg.t1; ++q, ++k) {
+        if (k >= cap) return CINTX_STATUS_BUFFER_TOO_SMALL;
+        const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
+        const int pa = t.rows[row], pb = t.cols[q - t.row_prefix[row]];
+        const Basis& B = o->basis;
+        quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
+        quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
+        quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
+        quartets[k * 4 + 3] = B.vshell[o->pair_b[pb]];
+      }
+    }
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+void cintx_plan_destroy(CintxPlan* p) {
+  if (!p) return;
+  free_plan_device(p);
+  delete p;
+}
+
+int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk) {
+  clear_error();
+  if (!plan) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  *plan = nullptr;
+  Opt* o = as_opt(optp);
+  if (!o) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "opt is not a handle created by this library");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  const Basis& B = o->basis;
+  if (B.nvirt != B.nbas) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "screened plans need single-contraction shells (nctr = 1)");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (B.env[PTR_RANGE_OMEGA] != 0.0) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "range-separated Coulomb is not supported");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (max_chunk <= 0) max_chunk = 1LL << 28;
+  const int np = o->npairs;
+  const int nb = B.nbas;
+  // 1. Schwarz factors from the diagonal (ij|ij) blocks, cartesian-free (sph) evaluation
+  std::vector<int> diag((size_t)np * 4);
+  for (int u = 0; u < nb; ++u)
+    for (int v = 0; v <= u; ++v) {
+      const int id = pair_index(u, v);
+      const int a = o->pair_a[id], b = o->pair_b[id];
+      int* d = &diag[(size_t)id * 4];
+      d[0] = a; d[1] = b; d[2] = a; d[3] = b;
+    }
+  std::vector<int64_t> doff(np);
+  CintxPlan* dp = nullptr;
+  int rc = cintx_plan_shells(&dp, optp, CINTX_INT2E, diag.data(), np, 1, doff.data());
+  if (rc) return rc;
+  std::vector<double> dout(std::max<int64_t>(dp->stats.nintegrals, 1));
+  rc = cintx_plan_execute_host(dp, 0, dout.data());
+  const long long dn = dp->stats.nintegrals;
+  cintx_plan_destroy(dp);
+  if (rc) return rc;
+  std::vector<double> Q(np, 0.0);
+  for (int id = 0; id < np; ++id) {
+    const long long e0 = doff[id], e1 = id + 1 < np ? doff[id + 1] : dn;
+    double m = 0;
+    for (long long e = e0; e < e1; ++e) m = std::max(m, fabs(dout[e]));
+    Q[id] = sqrt(m);
+  }
+  // 2. pair types (la, lb, nprim_a, nprim_b), sorted pairs by decreasing Q
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> types;
+  double qmax = 0;
+  for (int id = 0; id < np; ++id) qmax = std::max(qmax, Q[id]);
+  for (int id = 0; id < np; ++id) {
+    if (!(Q[id] * qmax >= cutoff) || o->pair_nprim[id] == 0) continue;
+    const int a = o->pair_a[id], b = o->pair_b[id];
+    types[std::make_tuple(o->pair_la[id], o->pair_lb[id], B.sh[a].nprim, B.sh[b].nprim)].push_back(id);
+  }
+  std::vector<std::vector<int>> tlist;
+  std::vector<std::tuple<int, int, int, int>> tkeys;
+  for (auto& kv : types) {
+    std::vector<int> v = kv.second;
+    std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return Q[x] > Q[y]; });
+    tlist.push_back(v);
+    tkeys.push_back(kv.first);
+  }
+  CintxPlan* p = new CintxPlan();
+  p->opt = o;
+  p->family = CINTX_INT2E;
+  p->sph = sph != 0;
+  const double ecut = expcutoff_2e(B.env.data());
+  long long nq_total = 0, nint_total = 0, nprimq = 0;
+  double flops = 0;
+  const int nt = (int)tlist.size();
+  // tiles A >= B in type order (types are ordered by (la, lb, ...), so classes are valid)
+  for (int A = 0; A < nt; ++A) {
+    for (int Bt = 0; Bt <= A; ++Bt) {
+      Tile t;
+      t.typeA = A;
+      t.typeB = Bt;
+      t.li = std::get<0>(tkeys[A]);
+      t.lj = std::get<1>(tkeys[A]);
+      t.lk = std::get<0>(tkeys[Bt]);
+      t.ll = std::get<1>(tkeys[Bt]);
+      const std::vector<int>& rows = tlist[A];
+      const std::vector<int>& cols = tlist[Bt];
+      std::vector<double> qcols(cols.size());
+      for (size_t c = 0; c < cols.size(); ++c) qcols[c] = Q[cols[c]];
+      std::vector<long long> cum_np(cols.size() + 1, 0);
+      for (size_t c = 0; c < cols.size(); ++c) cum_np[c + 1] = cum_np[c] + o->pair_nprim[cols[c]];
+      t.row_prefix.push_back(0);
+      for (size_t r = 0; r < rows.size(); ++r) {
+        const double qa = Q[rows[r]];
+        // count of cols with qa * Q >= cutoff (cols sorted decreasing)
+        long long cnt = std::partition_point(qcols.begin(), qcols.end(), [&](double qb) { return qa * qb >= cutoff; }) -
+                        qcols.begin();
+        if (A == Bt) cnt = std::min<long long>(cnt, (long long)r + 1);
+        if (cnt <= 0) continue;
+        t.rows.push_back(rows[r]);
+        t.row_prefix.push_back(t.row_prefix.back() + cnt);
+        nprimq += (long long)o->pair_nprim[rows[r]] * cum_np[cnt];
+      }
+      if (t.rows.empty()) continue;
+      t.cols = cols;
+      const long long nq = t.row_prefix.back();
+      const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
+                             nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
+      nq_total += nq;
+      nint_total += nq * nout;
+      p->tiles.push_back(t);
+    }
+  }
+  // flops: per tile class
+  {
+    // recompute nprim-weighted flops per tile
+    nprimq = 0;
+    for (const Tile& t : p->tiles) {
+      std::vector<long long> cum(t.cols.size() + 1, 0);
+      for (size_t c = 0; c < t.cols.size(); ++c) cum[c + 1] = cum[c] + o->pair_nprim[t.cols[c]];
+      long long tp = 0;
+      for (size_t r = 0; r < t.rows.size(); ++r) {
+        const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
+        tp += (long long)o->pair_nprim[t.rows[r]] * cum[cnt];
+      }
+      nprimq += tp;
+      const long long nq = t.row_prefix.back();
+      flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
+    }
+  }
+  // 3. chunks: greedy fill up to max_chunk doubles, splitting tiles at quartet boundaries
+  Chunk cur;
+  long long max_recs = 0;
+  for (int ti = 0; ti < (int)p->tiles.size(); ++ti) {
+    const Tile& t = p->tiles[ti];
+    const long long nq = t.row_prefix.back();
+    const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
+                           nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
+    long long q = 0;
+    while (q < nq) {
+      long long room = (max_chunk - cur.out_size) / nout;
+      if (room <= 0) {
+        if (cur.segs.empty()) room = 1;  // a single block larger than the chunk limit
+        else {
+          p->chunks.push_back(cur);
+          max_recs = std::max(max_recs, cur.nrec);
+          cur = Chunk();
+          continue;
+        }
+      }
+      const long long take = std::min(room, nq - q);
+      Segment sg;
+      sg.li = t.li;
+      sg.lj = t.lj;
+      sg.lk = t.lk;
+      sg.ll = t.ll;
+      sg.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
+      sg.expcutoff = ecut;
+      sg.tile = ti;
+      sg.t0 = q;
+      sg.t1 = q + take;
+      sg.nout = nout;
+      sg.rec0 = cur.nrec;
+      sg.out_off = cur.out_size;
+      cur.segs.push_back(sg);
+      cur.nrec += take;
+      cur.out_size += take * nout;
+      q += take;
+    }
+  }
+  if (!cur.segs.empty()) {
+    p->chunks.push_back(cur);
+    max_recs = std::max(max_recs, cur.nrec);
+  }
+  // 4. device buffers
+  p->rec_capacity = max_recs;
+  bool ok = true;
+  if (max_recs > 0) ok = cudaMalloc(&p->d_recs, sizeof(QuartetRec) * max_recs) == cudaSuccess;
+  for (Tile& t : p->tiles) {
+    if (!ok) break;
+    ok = cudaMalloc(&t.d_rows, sizeof(int) * t.rows.size()) == cudaSuccess &&
+         cudaMalloc(&t.d_cols, sizeof(int) * t.cols.size()) == cudaSuccess &&
+         cudaMalloc(&t.d_prefix, sizeof(long long) * t.row_prefix.size()) == cudaSuccess;
+    if (ok) {
+      cudaMemcpy(t.d_rows, t.rows.data(), sizeof(int) * t.rows.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(t.d_prefix, t.row_prefix.data(), sizeof(long long) * t.row_prefix.size(), cudaMemcpyHostToDevice);
+    }
+  }
+  if (!ok) {
+    free_plan_device(p);
+    delete p;
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the screened plan failed");
+    return CINTX_STATUS_ALLOCATION_FAILED;
+  }
+  long long maxc = 0;
+  for (const Chunk& c : p->chunks) maxc = std::max(maxc, c.out_size);
+  p->stats.nquartets = nq_total;
+  p->stats.nintegrals = nint_total;
+  p->stats.nchunks = (int64_t)p->chunks.size();
+  p->stats.max_chunk_doubles = maxc;
+  p->stats.nprim_quartets = nprimq;
+  p->stats.flops = flops;
+  *plan = p;
+  return CINTX_STATUS_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+/*
+ * cintx_cuda: B200 (sm_100a) two-electron Gaussian integrals behind libcint's C ABI.
+ *
+ * libcintx_cuda.so exports libcint 6.1.3's symbols for the Rys-quadrature Coulomb family so a
+ * caller that binds libcint (PySCF-style ctypes drivers, the cintx-compat legacy path, the
+ * cintx-oracle parity harness) can load this library instead.  Each libcint-signature entry
+ * point keeps libcint's argument meaning, output layout and return value:
+ *   - out == NULL  -> returns a cache size (in doubles) and computes nothing;
+ *   - dims == NULL -> block written as out[i + ni*(j + nj*(k + nk*l))], each axis indexed
+ *                     ctr*(2l+1)+m (sph) or ctr*ncart(l)+cart (cart), i.e. the layout of
+ *                     c2s_sph_2e1 / c2s_cart_2e1 (cint2e.c:794-870, cart2sph.c:5324);
+ *   - dims != NULL -> the same block placed in an array of extents dims[0..3];
+ *   - return value -> 1 if any primitive survived libcint's exponent screening
+ *                     (CINT2e_loop_nopt, cint2e.c:57), else 0 with the block zeroed.
+ * `cache` is accepted and ignored (device memory is managed by the library).  `opt` must be
+ * NULL or a handle made by this library's *_optimizer functions.
+ * Differences from libcint: range-separated Coulomb (env[PTR_RANGE_OMEGA] != 0) and shells
+ * with l > 4 are rejected (last error set, block zeroed, return 0) instead of computed, and
+ * Rys-root failures never call exit().
+ *
+ * FINT is int and CACHE_SIZE_T is int, as in libcint built without I8 (cint.h.in:10-24).
+ */
+#ifndef CINTX_CUDA_H
+#define CINTX_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CINTX_API __attribute__((visibility("default")))
+#else
+#define CINTX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CINTOpt CINTOpt; /* opaque here; libcint's is cint.h.in:136 */
+
+/* ---- libcint-signature entry points ---------------------------------------------------- */
+
+/* Replaces libcint int2e_sph (libcint-master/src/cint2e.c:1186) and, in cintx, the
+ * cintx-capi id-dispatch cintrs_eval(api=10) path (crates/cintx-capi/src/shim.rs:371). */
+CINTX_API int int2e_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+              double *env, CINTOpt *opt, double *cache);
+/* Replaces libcint int2e_cart (cint2e.c:1202); cintrs_eval api=9. */
+CINTX_API int int2e_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+               double *env, CINTOpt *opt, double *cache);
+/* Replaces libcint int2e_optimizer (cint2e.c:1195) and cintx-compat int2e_sph_optimizer
+ * (crates/cintx-compat/src/optimizer.rs:99).  Builds the device-resident basis and all
+ * screened primitive-pair tables once. */
+CINTX_API void int2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+
+/* Replaces libcint int2c2e_sph / int2c2e_cart / int2c2e_optimizer (cint2c2e.c:351-387);
+ * cintrs_eval api=13 / 12. */
+CINTX_API int int2c2e_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                double *env, CINTOpt *opt, double *cache);
+CINTX_API int int2c2e_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                 double *env, CINTOpt *opt, double *cache);
+CINTX_API void int2c2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+
+/* Replaces libcint int3c2e_sph / int3c2e_cart / int3c2e_optimizer (cint3c2e.c:693-718). */
+CINTX_API int int3c2e_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                double *env, CINTOpt *opt, double *cache);
+CINTX_API int int3c2e_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                 double *env, CINTOpt *opt, double *cache);
+CINTX_API void int3c2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+
+/* Replaces libcint CINTdel_optimizer (optimizer.c:69). Sets *opt to NULL. */
+CINTX_API void CINTdel_optimizer(CINTOpt **opt);
+
+/* Replaces libcint CINTrys_roots (rys_roots.c:57): u[r] = t_r^2/(1-t_r^2) and w[r] for
+ * order nroots (1..9), evaluated by the device root evaluator.  Returns 0 on success. */
+CINTX_API int CINTrys_roots(int nroots, double x, double *u, double *w);
+
+/* Device root evaluator over many points (no libcint counterpart; used to verify the root
+ * table): t2w[i*2n + r] = t_r^2 and t2w[i*2n + n + r] = w_r at x[i].  Host arrays. */
+CINTX_API int cintx_rys_t2_batch(int nroots, const double *x, int64_t nx, double *t2w);
+
+/* ---- status and last error (cintx-capi errors.rs:9-21, 98-139) ------------------------- */
+
+enum {
+  CINTX_STATUS_SUCCESS = 0,
+  CINTX_STATUS_INVALID_INPUT = 1,
+  CINTX_STATUS_UNSUPPORTED_API = 2,
+  CINTX_STATUS_UNSUPPORTED_REPRESENTATION = 3,
+  CINTX_STATUS_BUFFER_TOO_SMALL = 4,
+  CINTX_STATUS_MEMORY_LIMIT_EXCEEDED = 5,
+  CINTX_STATUS_ALLOCATION_FAILED = 6,
+  CINTX_STATUS_EXECUTION_FAILED = 7,
+  CINTX_STATUS_NULL_POINTER = 8,
+  CINTX_STATUS_PANIC = 9,
+  CINTX_STATUS_BACKEND_NOT_COMPILED = 10
+};
+
+/* Status of the calling thread's most recent failed call (0 if none); cleared by
+ * cintx_cuda_clear_last_error.  Mirrors cintrs_last_error_code (cintx-capi errors.rs). */
+CINTX_API int cintx_cuda_last_error_code(void);
+/* Copies the thread's last error message (NUL-terminated, truncated to cap). Returns the
+ * full message length.  Mirrors cintrs_copy_last_error_message. */
+CINTX_API size_t cintx_cuda_last_error_message(char *buf, size_t cap);
+CINTX_API void cintx_cuda_clear_last_error(void);
+
+/* ---- batched device API (no libcint counterpart; the path the B200 engine is built for) - */
+
+typedef struct CintxPlan CintxPlan;
+
+/* Integral family of a plan. */
+enum { CINTX_INT2E = 0, CINTX_INT3C2E = 1, CINTX_INT2C2E = 2 };
+
+/* Plan an explicit list of shell tuples (4 ints per int2e entry, 3 per int3c2e, 2 per
+ * int2c2e, host memory).  Output blocks are laid out back to back in list order, each in
+ * libcint's dims==NULL layout; offsets_out (host, n entries, may be NULL) receives each
+ * block's offset in doubles.  `opt` must come from the matching *_optimizer.  Returns a
+ * status code. */
+CINTX_API int cintx_plan_shells(CintxPlan **plan, CINTOpt *opt, int family, const int *shls, int64_t n,
+                      int sph, int64_t *offsets_out);
+
+/* Plan every 8-fold-unique int2e quartet (i>=j, k>=l, ij>=kl over pairs oriented and ordered
+ * by angular momentum) whose Schwarz bound sqrt(max|(ij|ij)| max|(kl|kl)|) reaches cutoff.
+ * The work is split into chunks whose outputs fit in max_chunk_doubles; chunk outputs are
+ * libcint-layout blocks back to back.  Returns a status code. */
+CINTX_API int cintx_plan_int2e_screened(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
+                              int64_t max_chunk_doubles);
+
+/* Plan statistics. */
+typedef struct {
+  int64_t nquartets;        /* shell tuples in the plan */
+  int64_t nintegrals;       /* output doubles over all chunks */
+  int64_t nchunks;
+  int64_t max_chunk_doubles;/* largest chunk output */
+  int64_t nprim_quartets;   /* primitive tuples surviving the pair screening */
+  double flops;             /* FP64 flops of the Rys path: per primitive quartet VRR 15*nroots*
+                               (li+lj+1)(lk+ll+1), HRR 6*nroots per transfer step, products
+                               3*nroots per cartesian element; per quartet the c2s stages */
+} CintxPlanStats;
+CINTX_API int cintx_plan_stats(const CintxPlan *plan, CintxPlanStats *stats);
+/* Output size (doubles) and tuple list of one chunk; quartets may be NULL. */
+CINTX_API int64_t cintx_plan_chunk_size(const CintxPlan *plan, int64_t chunk);
+CINTX_API int64_t cintx_plan_chunk_nquartets(const CintxPlan *plan, int64_t chunk);
+CINTX_API int cintx_plan_chunk_quartets(const CintxPlan *plan, int64_t chunk, int *quartets, int64_t cap);
+
+/* Run one chunk (or all chunks when chunk < 0, each overwriting out_dev) on `stream`
+ * (a cudaStream_t; NULL = the library's per-thread stream).  out_dev is device memory of
+ * at least the chunk size (all-chunk runs: max_chunk_doubles).  Asynchronous. */
+CINTX_API int cintx_plan_execute(CintxPlan *plan, int64_t chunk, double *out_dev, void *stream);
+/* Same, end to end: device output staged through a device ring and copied to host memory
+ * out_host (at least chunk size; all-chunk runs overwrite it per chunk).  Synchronous. */
+CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);
+CINTX_API void cintx_plan_destroy(CintxPlan *plan);
+
+/* Kernel launches issued by the calling thread's plan executions so far (for accounting). */
+CINTX_API int64_t cintx_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CINTX_CUDA_H */

@@ -1,0 +1,197 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and golden vectors.
+
+Tolerance is the reference's parity rule (cintx-oracle tests/two_electron_parity.rs:26-33):
+per element |d| <= 1e-12 or |d| <= 1e-10 |ref|.  Return values (screening) must match exactly.
+"""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, close
+from cintx_b200 import molecules as M
+from oracle import RefLibcint, Restatement
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.fixture(scope="module")
+def cx():
+    import cintx_b200
+    return cintx_b200
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Restatement()
+
+
+def test_device_roots_vs_mpmath(cx):
+    g = np.load(os.path.join(GOLD, "roots_mpmath.npz"))
+    for n in range(1, 10):
+        t2, w = cx.rys_t2_batch(n, g["x"])
+        np.testing.assert_allclose(t2, g["t2_%d" % n], rtol=5e-15, atol=0)
+        np.testing.assert_allclose(w, g["w_%d" % n], rtol=5e-15, atol=0)
+
+
+def test_cintrys_roots_convention(cx, orc):
+    rng = np.random.default_rng(3)
+    for n in range(1, 10):
+        for x in np.concatenate([rng.uniform(0, 120, 30), [0.0, 1e-12, 5e4]]):
+            u, w = cx.rys_roots(n, x)
+            uo, wo = orc.rys_roots(n, x)
+            np.testing.assert_allclose(u, uo, rtol=1e-13)
+            np.testing.assert_allclose(w, wo, rtol=1e-13)
+
+
+def test_int2e_sph_water3_all_quartets(cx, orc):
+    """Every one of the 12^4 quartets of the 3-atom molecule, per-call path, with and
+    without an optimizer handle."""
+    mol = M.water_like()
+    quartets = list(itertools.product(range(mol.nbas), repeat=4))
+    ref, offs = orc.int2e_batch(quartets, mol, sph=True)
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        for n, q in enumerate(quartets):
+            out, ret = cx.int2e_sph(q, mol.atm, mol.bas, mol.env, opt=opt if n % 2 else None)
+            r = ref[offs[n]:offs[n] + out.size]
+            _, rret = orc.int2e(q, mol)
+            assert ret == rret, q
+            assert close(out, r), (q, np.abs(out - r).max())
+
+
+def _golden_family(cx, mol, data, fam, fn, opt=None):
+    tup, offs, vals, rets = (data[fam + k] for k in ("_tuples", "_offsets", "_values", "_ret"))
+    for q, t in enumerate(tup):
+        out, ret = fn(t, mol.atm, mol.bas, mol.env, opt=opt)
+        ref = vals[offs[q]:offs[q + 1]]
+        assert ret == rets[q], (fam, t)
+        assert close(out, ref), (fam, t, np.abs(out - ref).max())
+
+
+def test_golden_water3_all_families(cx):
+    mol = M.water_like()
+    g = np.load(os.path.join(GOLD, "libcint_water3.npz"))
+    for fam in ("int2e_sph", "int2e_cart", "int3c2e_sph", "int3c2e_cart", "int2c2e_sph", "int2c2e_cart"):
+        _golden_family(cx, mol, g, fam, getattr(cx, fam))
+
+
+def test_golden_g_shells(cx):
+    mol = M.mol20_g()
+    g = np.load(os.path.join(GOLD, "libcint_mol20g.npz"))
+    _golden_family(cx, mol, g, "int2e_sph", cx.int2e_sph)
+
+
+def test_golden_general_contraction(cx):
+    g = np.load(os.path.join(GOLD, "libcint_ctr2.npz"))
+    mol = M.Molecule("ctr2", g["atm"], g["bas"], g["env"], np.zeros((2, 3)))
+    _golden_family(cx, mol, g, "int2e_sph", cx.int2e_sph)
+    _golden_family(cx, mol, g, "int2e_cart", cx.int2e_cart)
+    _golden_family(cx, mol, g, "int3c2e_sph", cx.int3c2e_sph)
+
+
+def test_dims_and_expcutoff(cx, orc):
+    mol = M.water_like()
+    q = (5, 0, 4, 3)  # (d s | p p): counts (5, 1, 3, 3)
+    ref, _ = orc.int2e(q, mol)
+    dims = (7, 2, 4, 5)
+    big = np.full(int(np.prod(dims)), 7.0)
+    out, ret = cx.int2e_sph(q, mol.atm, mol.bas, mol.env, dims=dims, out=big)
+    view = out.reshape(dims[::-1])  # [l][k][j][i]
+    np.testing.assert_allclose(view[:3, :3, :1, :5], ref.reshape(3, 3, 1, 5), atol=1e-12)
+    mask = np.ones(dims[::-1], dtype=bool)
+    mask[:3, :3, :1, :5] = False
+    assert np.all(view[mask] == 7.0)
+    # a tight exponent cut-off changes screening identically in oracle and device
+    env = mol.env.copy()
+    env[0] = 40.0
+    for t in [(0, 1, 0, 1), (0, 3, 6, 9), (5, 5, 11, 11)]:
+        m2 = M.Molecule("w", mol.atm, mol.bas, env, mol.coords)
+        a, ra = orc.int2e(t, m2)
+        b, rb = cx.int2e_sph(t, mol.atm, mol.bas, env)
+        assert ra == rb and close(b, a)
+
+
+@pytest.mark.parametrize("sph", [True, False])
+def test_explicit_plan_matches_per_call(cx, orc, sph):
+    mol = M.water_like()
+    rng = np.random.default_rng(11)
+    quartets = rng.integers(0, mol.nbas, size=(3000, 4)).astype(np.int32)
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.shells(opt, 0, quartets, sph=sph)
+        out = np.zeros(plan.stats.nintegrals)
+        plan.execute_host(out)
+        ref, offs = orc.int2e_batch(quartets, mol, sph=sph)
+        assert np.array_equal(plan.offsets, offs)
+        assert close(out, ref), np.abs(out - ref).max()
+        plan.close()
+    # 3- and 2-centre families through the same plan machinery
+    trip = rng.integers(0, mol.nbas, size=(500, 3)).astype(np.int32)
+    duo = rng.integers(0, mol.nbas, size=(100, 2)).astype(np.int32)
+    with cx.Optimizer(mol.atm, mol.bas, mol.env, family=1) as opt:
+        p3 = cx.Plan.shells(opt, 1, trip, sph=sph)
+        o3 = p3.execute_host(np.zeros(p3.stats.nintegrals))
+        p2 = cx.Plan.shells(opt, 2, duo, sph=sph)
+        o2 = p2.execute_host(np.zeros(p2.stats.nintegrals))
+        r3 = np.concatenate([orc.int3c2e(t, mol, sph)[0] for t in trip])
+        r2 = np.concatenate([orc.int2c2e(t, mol, sph)[0] for t in duo])
+        assert close(o3, r3) and close(o2, r2)
+        p3.close()
+        p2.close()
+
+
+def test_screened_plan_mol40(cx, orc):
+    """Schwarz-screened unique-quartet sweep: count, and every block of a seeded sample of
+    quartets checked against the oracle."""
+    mol = M.mol40()
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 26)
+        st = plan.stats
+        assert st.nchunks >= 1 and st.nquartets > 0
+        import torch
+        buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        rng = np.random.default_rng(5)
+        seen = 0
+        for c in range(st.nchunks):
+            plan.execute(buf.data_ptr(), chunk=c, stream=torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            quart = plan.chunk_quartets(c)
+            seen += len(quart)
+            if c % max(1, st.nchunks // 3):
+                continue
+            host = buf[:plan.chunk_size(c)].cpu().numpy()
+            sizes = np.array([orc_block(mol, q) for q in quart])
+            offs = np.concatenate([[0], np.cumsum(sizes)])
+            for k in rng.choice(len(quart), size=min(300, len(quart)), replace=False):
+                r, _ = orc.int2e(quart[k], mol)
+                assert close(host[offs[k]:offs[k + 1]], r), (c, quart[k])
+        assert seen == st.nquartets
+        plan.close()
+
+
+def orc_block(mol, q):
+    n = 1
+    for s in q:
+        n *= 2 * int(mol.bas[s, 1]) + 1
+    return n
+
+
+@pytest.mark.skipif(not RefLibcint.available(), reason="libcint from the reference sources not built")
+def test_against_live_libcint_mol40_sample(cx):
+    ref = RefLibcint()
+    mol = M.mol40()
+    rng = np.random.default_rng(9)
+    for t in rng.integers(0, mol.nbas, size=(400, 4)):
+        a, ra = cx.int2e_sph(t, mol.atm, mol.bas, mol.env)
+        b, rb = ref.int2e(t, mol)
+        assert ra == rb and close(a, b), t
+
+
+def test_unsupported_inputs_report_errors(cx):
+    mol = M.water_like()
+    env = mol.env.copy()
+    env[8] = 0.3  # range-separated Coulomb
+    with pytest.raises(cx.CintxError) as e:
+        cx.int2e_sph((0, 0, 0, 0), mol.atm, mol.bas, env)
+    assert e.value.code == 2
