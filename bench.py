@@ -1,0 +1,431 @@
+"""Benchmark: int2e_sph Gint/s on the seeded synthetic molecules, one JSON line on rank 0.
+
+A step is one full pass of the hot path over the workload: every 8-fold-unique shell quartet
+whose Schwarz bound reaches 1e-12 (cintx_plan_int2e_screened), evaluated into a device output
+ring chunk by chunk (libcint-layout blocks).  The pair tables are resident in HBM before the
+timed region; L2 is flushed (a 512 MiB write) between timed steps outside the step events.
+
+  value      Gint/s = spherical integrals written per second, device time (CUDA events on the
+             launching stream), max over ranks
+  e2e        the same metric through the C ABI from host arrays: optimizer build (host -> device
+             basis and pair tables), screened plan, execution and the device -> host copy of every
+             chunk's output into pinned host memory, every step
+  roofline   the kernel class with the largest device time in one profiled step: algorithmic FP64
+             flops (the plan's flop model) / its event time, against the FP64 FMA peak measured by
+             a probe kernel on the same GPU in the same run
+  cpu_baseline  libcint 6.1.3 built from the reference sources (oracle/_ref), all host cores,
+             on a seeded uniform sample of the same quartet set, extrapolated to the full set
+
+--impl reference times that libcint CPU path alone (rank 0) on the same workload and metric.
+Multi-GPU: chunks are distributed over ranks by their flop estimate (strong scaling: the
+total work is the molecule's quartet set, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cintx_b200 import molecules as M  # noqa: E402
+
+WORKLOADS = {
+    "mol40_spd": (M.mol40, "40 seeded atoms in a 14-bohr cube, 60% light (2s,1p) / 40% heavy "
+                           "(3s,2p,1d), exponents log-uniform [0.1,1.2e4]; Schwarz 1e-12"),
+    "mol120_spdf": (M.mol120, "120 seeded atoms in a 22-bohr cube, heavy atoms add one f shell; "
+                              "Schwarz 1e-12"),
+    "water3": (M.water_like, "3-atom water-like molecule (O + 2 H), all quartets above 1e-12"),
+}
+SCHWARZ = 1e-12
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cint_cpu_bench")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="mol40_spd", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chunk-doubles", type=int, default=1 << 27)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ CPU baseline (libcint)
+def write_driver_input(path, mol, quartets):
+    with open(path, "wb") as fh:
+        np.array([mol.natm, mol.nbas, mol.env.size, len(quartets)], dtype=np.int32).tofile(fh)
+        np.ascontiguousarray(mol.atm, dtype=np.int32).tofile(fh)
+        np.ascontiguousarray(mol.bas, dtype=np.int32).tofile(fh)
+        np.ascontiguousarray(mol.env, dtype=np.float64).tofile(fh)
+        np.ascontiguousarray(quartets, dtype=np.int32).tofile(fh)
+
+
+def run_libcint(mol, quartets, threads):
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "in.bin")
+        write_driver_input(p, mol, quartets)
+        r = subprocess.run([REF_DRIVER, p, str(threads)], capture_output=True, text=True, check=True)
+    return json.loads(r.stdout)
+
+
+def cpu_rate(mol, sampler, nq_total, nint_total, seconds, threads):
+    """libcint time per quartet on a seeded uniform sample, extrapolated to the full set."""
+    n = 2000
+    res = run_libcint(mol, sampler(n, 1), threads)
+    per_q = res["seconds"] / n
+    n = int(min(5_000_000, max(n, seconds / max(per_q, 1e-9))))
+    res = run_libcint(mol, sampler(n, 2), threads)
+    per_q = res["seconds"] / n
+    full_s = per_q * nq_total
+    return {"value": nint_total / full_s / 1e9, "unit": "Gint/s", "cores": int(res["threads"]),
+            "kind": "reference",
+            "sample": "%d quartets drawn uniformly (seeded) from the %d-quartet set, %.1f s of libcint "
+                      "int2e_sph with an optimizer, OpenMP dynamic; extrapolated by quartet count" %
+                      (n, nq_total, res["seconds"]),
+            "seconds": res["seconds"]}
+
+
+# ------------------------------------------------------------------ reference arm
+def schwarz_pairs_libcint(mol):
+    """Q_ij = sqrt(max |(ij|ij)|) for all pairs i >= j, with libcint on the CPU."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import RefLibcint
+    ref = RefLibcint()
+    pairs = [(i, j) for i in range(mol.nbas) for j in range(i + 1)]
+
+    def one(p):
+        out, _ = ref.int2e((p[0], p[1], p[0], p[1]), mol)
+        return np.sqrt(np.abs(out).max())
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        q = np.array(list(ex.map(one, pairs, chunksize=256)))
+    return np.array(pairs, dtype=np.int32), q
+
+
+class UniqueQuartets:
+    """The plan's quartet set (unordered pairs of shell pairs with Q_p Q_q >= cutoff), built on
+    the host from libcint Schwarz factors, with uniform sampling."""
+
+    def __init__(self, mol, cutoff):
+        self.mol = mol
+        pairs, q = schwarz_pairs_libcint(mol)
+        order = np.argsort(-q, kind="stable")
+        self.pairs, self.q = pairs[order], q[order]
+        keep = self.q * self.q.max() >= cutoff
+        self.pairs, self.q = self.pairs[keep], self.q[keep]
+        thr = cutoff / np.maximum(self.q, 1e-300)
+        # number of partners j <= i (sorted decreasing) with q_j >= cutoff / q_i
+        L = np.searchsorted(-self.q, -thr, side="right")
+        self.count = np.minimum(np.arange(len(self.q)) + 1, L)
+        l = mol.bas[:, 1]
+        ns = (2 * l[self.pairs[:, 0]] + 1) * (2 * l[self.pairs[:, 1]] + 1)
+        cum = np.concatenate([[0], np.cumsum(ns)])
+        self.nquartets = int(self.count.sum())
+        self.nintegrals = int((ns * cum[self.count]).sum())
+        self.prob = self.count / self.count.sum()
+
+    def sample(self, n, seed):
+        rng = np.random.default_rng(seed)
+        i = rng.choice(len(self.q), size=n, p=self.prob)
+        j = (rng.random(n) * self.count[i]).astype(np.int64)
+        return np.concatenate([self.pairs[i], self.pairs[j]], axis=1).astype(np.int32)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fn, desc = WORKLOADS[args.workload]
+    if not os.path.exists(REF_DRIVER):
+        print(json.dumps({"impl": "reference", "unavailable": "libcint was not built from the reference "
+                          "sources (oracle/_ref missing)"}))
+        return
+    mol = fn()
+    uq = UniqueQuartets(mol, SCHWARZ)
+    threads = os.cpu_count() or 1
+    # per-step sample sized for ~target seconds
+    cal = run_libcint(mol, uq.sample(2000, 100), threads)
+    per_q = cal["seconds"] / 2000
+    nsamp = int(min(2_000_000, max(2000, 8.0 / max(per_q, 1e-9))))
+    times = []
+    for s in range(args.warmup + args.steps):
+        res = run_libcint(mol, uq.sample(nsamp, 1000 + s), threads)
+        if s >= args.warmup:
+            times.append(res["seconds"] / nsamp * uq.nquartets)  # extrapolated full-step time
+    t = statistics.mean(times)
+    value = uq.nintegrals / t / 1e9
+    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (libcint CPU reference)", "value": value,
+            "unit": "Gint/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": args.workload, "description": desc, "nquartets": uq.nquartets,
+                       "nintegrals": uq.nintegrals, "schwarz_cutoff": SCHWARZ},
+            "cpu_baseline": {"value": value, "unit": "Gint/s", "cores": threads, "kind": "reference",
+                             "sample": "%d seeded uniform quartets per step, extrapolated by quartet count" % nsamp},
+            "e2e": {"value": value, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+def fp64_peak(cx, torch):
+    """FP64 FMA pipe throughput of this GPU (TFLOP/s), best of 3."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, threads, iters = sms * 8, 256, 2000
+    out = torch.empty(blocks * threads, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = cx.lib.cintx_fp64_fma_probe(blocks, threads, iters, out.data_ptr(), st.cuda_stream)
+        e1.record()
+        e1.synchronize()
+        assert rc == 0
+        flops = blocks * threads * iters * 16 * 8 * 2.0
+        best = max(best, flops / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def balance(costs, nranks):
+    """Greedy longest-processing-time assignment of chunks to ranks."""
+    order = sorted(range(len(costs)), key=lambda c: -costs[c])
+    load = [0.0] * nranks
+    owner = [0] * len(costs)
+    for c in order:
+        r = min(range(nranks), key=lambda k: load[k])
+        owner[c] = r
+        load[r] += costs[c]
+    return owner
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import cintx_b200 as cx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    fn, desc = WORKLOADS[args.workload]
+    mol = fn()
+    opt = cx.Optimizer(mol.atm, mol.bas, mol.env)
+    plan = cx.Plan.screened(opt, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
+    st = plan.stats
+    nchunks = st.nchunks
+    seg_info = [plan.segments(c) for c in range(nchunks)]
+    chunk_flops = [float(s[2].sum()) for s in seg_info]
+    owner = balance(chunk_flops, world)
+    mine = [c for c in range(nchunks) if owner[c] == rank]
+    my_ints = sum(plan.chunk_size(c) for c in mine)
+    stream = torch.cuda.current_stream()
+    ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        for c in mine:
+            plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = cx.launch_count()
+    t_wall = time.perf_counter()
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_wall = time.perf_counter() - t_wall
+    launches = cx.launch_count() - launches0
+    clk = clocks.stop()
+    dev_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
+
+    # per-class profile of one step (segments timed individually)
+    per_class = {}
+    for c in mine:
+        cls, nq, fl = seg_info[c]
+        for s in range(len(nq)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.execute_segment(ring.data_ptr(), c, s, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            key = "(%d%d|%d%d)" % tuple(cls[s])
+            d = per_class.setdefault(key, {"ms": 0.0, "flops": 0.0, "quartets": 0, "launches": 0})
+            d["ms"] += e0.elapsed_time(e1)
+            d["flops"] += float(fl[s])
+            d["quartets"] += int(nq[s])
+            d["launches"] += 1
+    peak64 = fp64_peak(cx, torch)
+    top = max(per_class.items(), key=lambda kv: kv[1]["ms"]) if per_class else (None, None)
+    roof = None
+    if top[0] is not None:
+        d = top[1]
+        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
+        prof_total = sum(v["ms"] for v in per_class.values())
+        roof = {"bound": "fp64", "kernel": "eri4c_kernel" + top[0], "achieved": achieved, "peak": peak64,
+                "unit": "TFLOP/s", "frac": achieved / peak64,
+                "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "share_of_step": d["ms"] / prof_total, "traffic": None,
+                "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    hbm = None
+    try:
+        hbm = json.load(open(PEAKS_FILE))["hbm_gbs"]
+    except Exception:
+        pass
+    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (plain FP64 form)", "value": value, "unit": "Gint/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded molecule; no dataset)",
+            "config": {"workload": args.workload, "description": desc, "form": "plain_fp64",
+                       "nquartets": st.nquartets, "nintegrals": st.nintegrals, "nchunks": nchunks,
+                       "chunk_doubles": args.chunk_doubles, "schwarz_cutoff": SCHWARZ,
+                       "nprim_quartets": st.nprim_quartets, "model_flops_per_step": st.flops,
+                       "l2": "flushed between steps (512 MiB write outside the step events); each step also "
+                             "streams %.1f GB of output through HBM" % (st.nintegrals * 8 / 1e9)},
+            "quartets_per_s": st.nquartets / (ms_per_step * 1e-3),
+            "gpu_launches": launches,
+            "clocks": clk, "wall_s_timed_region": t_wall,
+            "roofline": roof,
+            "output_write_gbs": st.nintegrals * 8 / (ms_per_step * 1e-3) / 1e9,
+            "hbm_gbs_measured_peak": hbm,
+            "per_class_ms": {k: round(v["ms"], 3) for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:12]}}
+
+    # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1)
+    if not args.no_e2e:
+        host = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, pin_memory=True).numpy()
+        e2e_times = []
+        h2d = d2h = 0
+        for s in range(1 + max(1, min(args.steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env)
+            p2 = cx.Plan.screened(o2, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
+            for c in mine:
+                p2.execute_host(host, chunk=c)
+            t1 = time.perf_counter()
+            if s > 0:
+                e2e_times.append(t1 - t0)
+            h2d = o2.device_bytes + p2.stats.device_bytes + mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes
+            d2h = my_ints * 8
+            p2.close()
+            o2.close()
+        te = statistics.mean(e2e_times)
+        line["e2e"] = {"value": st.nintegrals / te / 1e9 if world == 1 else my_ints / te / 1e9 * world,
+                       "unit": "Gint/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "seconds_per_step": te,
+                       "includes": "int2e_optimizer + screened plan (Schwarz pass) + execution + D2H of every chunk"}
+    if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
+        line["cpu_baseline"] = cpu_rate(mol, lambda n, seed: plan.sample_quartets(n, seed), st.nquartets,
+                                        st.nintegrals, args.cpu_seconds, os.cpu_count() or 1)
+    elif world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = None
+    print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    plan.close()
+    opt.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

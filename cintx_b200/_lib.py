@@ -26,7 +26,8 @@ class CintxError(RuntimeError):
 
 class PlanStats(ctypes.Structure):
     _fields_ = [("nquartets", _i64), ("nintegrals", _i64), ("nchunks", _i64),
-                ("max_chunk_doubles", _i64), ("nprim_quartets", _i64), ("flops", _d)]
+                ("max_chunk_doubles", _i64), ("nprim_quartets", _i64), ("device_bytes", _i64),
+                ("flops", _d)]
 
 
 def _load() -> ctypes.CDLL:
@@ -72,6 +73,16 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_destroy.argtypes = [_vp]
     L.cintx_plan_destroy.restype = None
     L.cintx_launch_count.restype = _i64
+    L.cintx_plan_chunk_segments.argtypes = [_vp, _i64, _ip, _i64p, _dp, _i]
+    L.cintx_plan_chunk_segments.restype = _i
+    L.cintx_plan_execute_segment.argtypes = [_vp, _i64, _i, _vp, _vp]
+    L.cintx_plan_execute_segment.restype = _i
+    L.cintx_plan_sample_quartets.argtypes = [_vp, ctypes.c_uint64, _i64, _ip]
+    L.cintx_plan_sample_quartets.restype = _i
+    L.cintx_opt_device_bytes.argtypes = [_vp]
+    L.cintx_opt_device_bytes.restype = _i64
+    L.cintx_fp64_fma_probe.argtypes = [_i, _i, _i, _vp, _vp]
+    L.cintx_fp64_fma_probe.restype = _i
     return L
 
 
@@ -180,6 +191,10 @@ class Optimizer:
         if not self.handle:
             raise CintxError(*last_error())
 
+    @property
+    def device_bytes(self) -> int:
+        return int(lib.cintx_opt_device_bytes(self.handle))
+
     def close(self):
         if self.handle:
             lib.CINTdel_optimizer(ctypes.byref(self.handle))
@@ -237,6 +252,24 @@ class Plan:
         n = int(lib.cintx_plan_chunk_nquartets(self.handle, chunk))
         q = np.zeros((max(n, 0), 4), dtype=np.int32)
         _check(lib.cintx_plan_chunk_quartets(self.handle, chunk, q.ctypes.data_as(_ip), n))
+        return q
+
+    def segments(self, chunk: int):
+        n = lib.cintx_plan_chunk_segments(self.handle, chunk, None, None, None, 0)
+        cls = np.zeros((max(n, 0), 4), dtype=np.int32)
+        nq = np.zeros(max(n, 0), dtype=np.int64)
+        fl = np.zeros(max(n, 0))
+        lib.cintx_plan_chunk_segments(self.handle, chunk, cls.ctypes.data_as(_ip), nq.ctypes.data_as(_i64p),
+                                      fl.ctypes.data_as(_dp), n)
+        return cls, nq, fl
+
+    def execute_segment(self, out_ptr: int, chunk: int, seg: int, stream: int = 0):
+        _check(lib.cintx_plan_execute_segment(self.handle, chunk, seg, ctypes.c_void_p(out_ptr),
+                                              ctypes.c_void_p(stream)))
+
+    def sample_quartets(self, n: int, seed: int = 0) -> np.ndarray:
+        q = np.zeros((n, 4), dtype=np.int32)
+        _check(lib.cintx_plan_sample_quartets(self.handle, seed, n, q.ctypes.data_as(_ip)))
         return q
 
     def execute(self, out_ptr: int, chunk: int = -1, stream: int = 0):

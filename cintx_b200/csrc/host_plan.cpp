@@ -43,6 +43,7 @@ struct Segment {
   long long t0 = 0, t1 = 0;
   long long nout = 0;      // doubles per block (screened)
   long long out_off = 0;   // chunk-relative output start of this segment
+  double flops = 0;        // algorithmic FP64 flops of the segment
 };
 
 struct Chunk {
@@ -56,6 +57,7 @@ struct Tile {
   int li, lj, lk, ll;
   std::vector<int> rows, cols;          // pair ids
   std::vector<long long> row_prefix;    // size rows+1
+  std::vector<long long> cum_np;        // prefix of primitive-pair counts over cols
   int* d_rows = nullptr;
   int* d_cols = nullptr;
   long long* d_prefix = nullptr;
@@ -151,6 +153,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   };
   std::map<GKey, std::vector<QuartetRec>> groups;
   std::map<GKey, std::vector<int>> group_tuples;
+  std::map<GKey, double> group_flops;
   long long off = 0;
   double flops = 0;
   long long nprimq = 0;
@@ -246,8 +249,10 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
             for (int a = 0; a < 4; ++a) group_tuples[k].push_back(rs[a]);
             const long long npq = (long long)o->pair_nprim[r.pij] * o->pair_nprim[r.pkl];
             nprimq += npq;
-            flops += npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
-                     flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
+            const double fq = npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
+                              flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
+            flops += fq;
+            group_flops[k] += fq;
           }
     off += blk;
   }
@@ -267,6 +272,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     sg.rec0 = rec0;
     sg.nrec = (long long)kv.second.size();
     sg.out_off = 0;
+    sg.flops = group_flops[kv.first];
     ch.segs.push_back(sg);
     p->h_recs.insert(p->h_recs.end(), kv.second.begin(), kv.second.end());
     auto& tu = group_tuples[kv.first];
@@ -291,68 +297,89 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   p->stats.max_chunk_doubles = off;
   p->stats.nprim_quartets = nprimq;
   p->stats.flops = flops;
+  p->stats.device_bytes = (int64_t)(sizeof(QuartetRec) * rec0);
   *plan = p;
+  return CINTX_STATUS_SUCCESS;
+}
+
+static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStream_t stream, DeviceState* ds,
+                       ThreadScratch* ts) {
+  const Opt* o = p->opt;
+  const QuartetRec* recs;
+  long long nrec;
+  if (sg.tile < 0) {
+    recs = p->d_recs + sg.rec0;
+    nrec = sg.nrec;
+  } else {
+    const Tile& t = p->tiles[sg.tile];
+    QuartetRec* dst = p->d_recs + sg.rec0;
+    cudaError_t e = launch_gen_tile(t.d_rows, t.d_cols, t.d_prefix, (int)t.rows.size(), sg.t0, sg.t1, sg.nout, 0,
+                                    dst, stream);
+    if (e != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("quartet generation failed: ") + cudaGetErrorString(e));
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+    ts->launches++;
+    recs = dst;
+    nrec = sg.t1 - sg.t0;
+  }
+  // the kernels take an int count; split very large segments
+  for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
+    const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
+    cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
+                                 out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream);
+    if (e != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+    ts->launches++;
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+static int exec_prepare(CintxPlan* p, double* out_dev, void* stream_, cudaStream_t* stream, DeviceState** ds,
+                        ThreadScratch** ts) {
+  if (!p || !out_dev) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and out_dev must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  int rc;
+  if ((rc = device_state(ds))) return rc;
+  if ((rc = thread_scratch(ts, 0, 0))) return rc;
+  *stream = stream_ ? (cudaStream_t)stream_ : (*ts)->stream;
   return CINTX_STATUS_SUCCESS;
 }
 
 int cintx_plan_execute(CintxPlan* p, int64_t chunk, double* out_dev, void* stream_) {
   clear_error();
-  if (!p || !out_dev) {
-    set_error(CINTX_STATUS_NULL_POINTER, "plan and out_dev must not be NULL");
-    return CINTX_STATUS_NULL_POINTER;
-  }
+  cudaStream_t stream;
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc = exec_prepare(p, out_dev, stream_, &stream, &ds, &ts);
+  if (rc) return rc;
   if (chunk >= (int64_t)p->chunks.size()) {
     set_error(CINTX_STATUS_INVALID_INPUT, "chunk index out of range");
     return CINTX_STATUS_INVALID_INPUT;
   }
-  DeviceState* ds;
-  int rc;
-  if ((rc = device_state(&ds))) return rc;
-  cudaStream_t stream = (cudaStream_t)stream_;
-  if (!stream) {
-    ThreadScratch* ts;
-    if ((rc = thread_scratch(&ts, 0, 0))) return rc;
-    stream = ts->stream;
-  }
-  ThreadScratch* ts;
-  if ((rc = thread_scratch(&ts, 0, 0))) return rc;
-  const Opt* o = p->opt;
   const int64_t c0 = chunk < 0 ? 0 : chunk, c1 = chunk < 0 ? (int64_t)p->chunks.size() : chunk + 1;
-  for (int64_t c = c0; c < c1; ++c) {
-    const Chunk& ch = p->chunks[c];
-    for (const Segment& sg : ch.segs) {
-      const QuartetRec* recs;
-      long long nrec;
-      if (sg.tile < 0) {
-        recs = p->d_recs + sg.rec0;
-        nrec = sg.nrec;
-      } else {
-        const Tile& t = p->tiles[sg.tile];
-        QuartetRec* dst = p->d_recs + sg.rec0;
-        cudaError_t e = launch_gen_tile(t.d_rows, t.d_cols, t.d_prefix, (int)t.rows.size(), sg.t0, sg.t1, sg.nout, 0,
-                                        dst, stream);
-        if (e != cudaSuccess) {
-          set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("quartet generation failed: ") + cudaGetErrorString(e));
-          return CINTX_STATUS_EXECUTION_FAILED;
-        }
-        ts->launches++;
-        recs = dst;
-        nrec = sg.t1 - sg.t0;
-      }
-      // the kernels take an int count; split very large segments
-      for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
-        const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
-        cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
-                                     out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream);
-        if (e != cudaSuccess) {
-          set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
-          return CINTX_STATUS_EXECUTION_FAILED;
-        }
-        ts->launches++;
-      }
-    }
-  }
+  for (int64_t c = c0; c < c1; ++c)
+    for (const Segment& sg : p->chunks[c].segs)
+      if ((rc = run_segment(p, sg, out_dev, stream, ds, ts))) return rc;
   return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_execute_segment(CintxPlan* p, int64_t chunk, int seg, double* out_dev, void* stream_) {
+  clear_error();
+  cudaStream_t stream;
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc = exec_prepare(p, out_dev, stream_, &stream, &ds, &ts);
+  if (rc) return rc;
+  if (chunk < 0 || chunk >= (int64_t)p->chunks.size() || seg < 0 || seg >= (int)p->chunks[chunk].segs.size()) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "chunk or segment index out of range");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  return run_segment(p, p->chunks[chunk].segs[seg], out_dev, stream, ds, ts);
 }
 
 int cintx_plan_execute_host(CintxPlan* p, int64_t chunk, double* out_host) {
@@ -432,6 +459,63 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
         quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
         quartets[k * 4 + 3] = B.vshell[o->pair_b[pb]];
       }
+    }
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_chunk_segments(const CintxPlan* p, int64_t chunk, int* cls, int64_t* nq, double* flops, int cap) {
+  if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return -1;
+  const Chunk& ch = p->chunks[chunk];
+  const int n = (int)ch.segs.size();
+  for (int s = 0; s < n && s < cap; ++s) {
+    const Segment& sg = ch.segs[s];
+    if (cls) {
+      cls[4 * s] = sg.li;
+      cls[4 * s + 1] = sg.lj;
+      cls[4 * s + 2] = sg.lk;
+      cls[4 * s + 3] = sg.ll;
+    }
+    if (nq) nq[s] = sg.tile < 0 ? sg.nrec : sg.t1 - sg.t0;
+    if (flops) flops[s] = sg.flops;
+  }
+  return n;
+}
+
+int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int* quartets) {
+  if (!p || !quartets || n < 0) return CINTX_STATUS_NULL_POINTER;
+  const Opt* o = p->opt;
+  const Basis& B = o->basis;
+  uint64_t st = seed;
+  auto next = [&]() {  // splitmix64
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  if (!p->tiles.empty()) {
+    std::vector<long long> tp(p->tiles.size() + 1, 0);
+    for (size_t t = 0; t < p->tiles.size(); ++t) tp[t + 1] = tp[t] + p->tiles[t].row_prefix.back();
+    const long long total = tp.back();
+    for (int64_t k = 0; k < n; ++k) {
+      const long long g = (long long)(next() % (uint64_t)total);
+      const size_t ti = std::upper_bound(tp.begin(), tp.end(), g) - tp.begin() - 1;
+      const Tile& t = p->tiles[ti];
+      const long long q = g - tp[ti];
+      const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
+      const int pa = t.rows[row], pb = t.cols[q - t.row_prefix[row]];
+      quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
+      quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
+      quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
+      quartets[k * 4 + 3] = B.vshell[o->pair_b[pb]];
+    }
+  } else {
+    const long long total = (long long)p->h_tuples.size() / 4;
+    if (total == 0) return CINTX_STATUS_INVALID_INPUT;
+    for (int64_t k = 0; k < n; ++k) {
+      const long long g = (long long)(next() % (uint64_t)total);
+      for (int a = 0; a < 4; ++a) quartets[k * 4 + a] = p->h_tuples[g * 4 + a];
     }
   }
   return CINTX_STATUS_SUCCESS;
@@ -547,6 +631,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       }
       if (t.rows.empty()) continue;
       t.cols = cols;
+      t.cum_np = cum_np;
       const long long nq = t.row_prefix.back();
       const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
                              nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
@@ -606,6 +691,21 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       sg.nout = nout;
       sg.rec0 = cur.nrec;
       sg.out_off = cur.out_size;
+      {
+        // flops of quartets [q, q + take): rows overlapping the range
+        double fl = 0;
+        const double fpp = flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll);
+        long long r = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
+        long long pos = q;
+        while (pos < q + take) {
+          const long long rend = std::min(t.row_prefix[r + 1], q + take);
+          const long long c0 = pos - t.row_prefix[r], c1 = rend - t.row_prefix[r];
+          fl += (double)o->pair_nprim[t.rows[r]] * (double)(t.cum_np[c1] - t.cum_np[c0]) * fpp;
+          pos = rend;
+          ++r;
+        }
+        sg.flops = fl + take * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
+      }
       cur.segs.push_back(sg);
       cur.nrec += take;
       cur.out_size += take * nout;
@@ -645,8 +745,20 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
   p->stats.max_chunk_doubles = maxc;
   p->stats.nprim_quartets = nprimq;
   p->stats.flops = flops;
+  {
+    long long db = (long long)sizeof(QuartetRec) * max_recs;
+    for (const Tile& t : p->tiles)
+      db += (long long)(sizeof(int) * (t.rows.size() + t.cols.size()) + sizeof(long long) * t.row_prefix.size());
+    p->stats.device_bytes = db;
+  }
   *plan = p;
   return CINTX_STATUS_SUCCESS;
+}
+
+int64_t cintx_opt_device_bytes(CINTOpt* optp) {
+  Opt* o = as_opt(optp);
+  if (!o) return -1;
+  return (int64_t)(sizeof(ShellPair) * (o->npairs + o->basis.nvirt) + sizeof(PrimPair) * o->nprims_total);
 }
 
 }  // extern "C"

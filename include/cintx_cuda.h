@@ -123,6 +123,9 @@ CINTX_API int cintx_plan_shells(CintxPlan **plan, CINTOpt *opt, int family, cons
 CINTX_API int cintx_plan_int2e_screened(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
                               int64_t max_chunk_doubles);
 
+/* Device bytes held by an optimizer handle (pair and primitive-pair tables). */
+CINTX_API int64_t cintx_opt_device_bytes(CINTOpt *opt);
+
 /* Plan statistics. */
 typedef struct {
   int64_t nquartets;        /* shell tuples in the plan */
@@ -130,6 +133,7 @@ typedef struct {
   int64_t nchunks;
   int64_t max_chunk_doubles;/* largest chunk output */
   int64_t nprim_quartets;   /* primitive tuples surviving the pair screening */
+  int64_t device_bytes;     /* device memory held by the plan (records, tile tables) */
   double flops;             /* FP64 flops of the Rys path: per primitive quartet VRR 15*nroots*
                                (li+lj+1)(lk+ll+1), HRR 6*nroots per transfer step, products
                                3*nroots per cartesian element; per quartet the c2s stages */
@@ -140,6 +144,17 @@ CINTX_API int64_t cintx_plan_chunk_size(const CintxPlan *plan, int64_t chunk);
 CINTX_API int64_t cintx_plan_chunk_nquartets(const CintxPlan *plan, int64_t chunk);
 CINTX_API int cintx_plan_chunk_quartets(const CintxPlan *plan, int64_t chunk, int *quartets, int64_t cap);
 
+/* Segments of a chunk: each is one kernel class over a contiguous run of quartets.  For
+ * segment s: cls[4s..4s+3] = (li, lj, lk, ll) of the kernel, nq[s] quartets, flops[s] the
+ * algorithmic FP64 flops (model of cintx_plan_stats).  Returns the segment count (or -1). */
+CINTX_API int cintx_plan_chunk_segments(const CintxPlan *plan, int64_t chunk, int *cls, int64_t *nq,
+                                        double *flops, int cap);
+/* Runs one segment of a chunk into out_dev (chunk-relative offsets, as cintx_plan_execute). */
+CINTX_API int cintx_plan_execute_segment(CintxPlan *plan, int64_t chunk, int seg, double *out_dev,
+                                         void *stream);
+/* n shell quartets drawn uniformly (with replacement, seeded) from the whole plan. */
+CINTX_API int cintx_plan_sample_quartets(const CintxPlan *plan, uint64_t seed, int64_t n, int *quartets);
+
 /* Run one chunk (or all chunks when chunk < 0, each overwriting out_dev) on `stream`
  * (a cudaStream_t; NULL = the library's per-thread stream).  out_dev is device memory of
  * at least the chunk size (all-chunk runs: max_chunk_doubles).  Asynchronous. */
@@ -148,6 +163,10 @@ CINTX_API int cintx_plan_execute(CintxPlan *plan, int64_t chunk, double *out_dev
  * out_host (at least chunk size; all-chunk runs overwrite it per chunk).  Synchronous. */
 CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);
 CINTX_API void cintx_plan_destroy(CintxPlan *plan);
+
+/* FP64 FMA throughput probe (measurement only): blocks x threads threads each run
+ * iters*16*8 FMAs and write one double to out_dev[blocks*threads].  Asynchronous on stream. */
+CINTX_API int cintx_fp64_fma_probe(int blocks, int threads, int iters, double *out_dev, void *stream);
 
 /* Kernel launches issued by the calling thread's plan executions so far (for accounting). */
 CINTX_API int64_t cintx_launch_count(void);
