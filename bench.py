@@ -57,7 +57,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="mol40_spd", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--chunk-doubles", type=int, default=1 << 27)
+    ap.add_argument("--chunk-doubles", type=int, default=1 << 28)
+    ap.add_argument("--branches", type=int, default=4)
+    ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -288,9 +290,19 @@ def our_arm(args):
     ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
+    use_graph = not args.no_graph
+    if use_graph:
+        try:
+            plan.graph_build(ring.data_ptr(), chunks=mine, nbranch=args.branches)
+        except cx.CintxError:
+            use_graph = False
+
     def step():
-        for c in mine:
-            plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
+        if use_graph:
+            plan.graph_launch(stream.cuda_stream)
+        else:
+            for c in mine:
+                plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -336,11 +348,12 @@ def our_arm(args):
             e1.record(stream)
             e1.synchronize()
             key = "(%d%d|%d%d)" % tuple(cls[s])
-            d = per_class.setdefault(key, {"ms": 0.0, "flops": 0.0, "quartets": 0, "launches": 0})
+            d = per_class.setdefault(key, {"ms": 0.0, "flops": 0.0, "quartets": 0, "launches": 0, "ints": 0})
             d["ms"] += e0.elapsed_time(e1)
             d["flops"] += float(fl[s])
             d["quartets"] += int(nq[s])
             d["launches"] += 1
+            d["ints"] += int(nq[s]) * int(np.prod([2 * l + 1 for l in cls[s]]))
     peak64 = fp64_peak(cx, torch)
     top = max(per_class.items(), key=lambda kv: kv[1]["ms"]) if per_class else (None, None)
     roof = None
@@ -380,7 +393,12 @@ def our_arm(args):
             "roofline": roof,
             "output_write_gbs": st.nintegrals * 8 / (ms_per_step * 1e-3) / 1e9,
             "hbm_gbs_measured_peak": hbm,
-            "per_class_ms": {k: round(v["ms"], 3) for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:12]}}
+            "execution": "one CUDA graph per step (%d kernel classes on %d branches)" % (len(per_class), args.branches)
+                         if use_graph else "direct launches",
+            "per_class": {k: {"ms": round(v["ms"], 4), "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3),
+                              "gint_s": round(v["ints"] / (v["ms"] * 1e-3) / 1e9, 2), "quartets": v["quartets"]}
+                          for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:16]},
+            "profiled_step_ms": sum(v["ms"] for v in per_class.values())}
 
     # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1)
     if not args.no_e2e:

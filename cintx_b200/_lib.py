@@ -79,6 +79,10 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute_segment.restype = _i
     L.cintx_plan_sample_quartets.argtypes = [_vp, ctypes.c_uint64, _i64, _ip]
     L.cintx_plan_sample_quartets.restype = _i
+    L.cintx_plan_graph_build.argtypes = [_vp, _i64p, _i64, _vp, _i]
+    L.cintx_plan_graph_build.restype = _i
+    L.cintx_plan_graph_launch.argtypes = [_vp, _vp]
+    L.cintx_plan_graph_launch.restype = _i
     L.cintx_opt_device_bytes.argtypes = [_vp]
     L.cintx_opt_device_bytes.restype = _i64
     L.cintx_fp64_fma_probe.argtypes = [_i, _i, _i, _vp, _vp]
@@ -275,6 +279,17 @@ class Plan:
     def execute(self, out_ptr: int, chunk: int = -1, stream: int = 0):
         """Asynchronous device execution into device pointer out_ptr."""
         _check(lib.cintx_plan_execute(self.handle, chunk, ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)))
+
+    def graph_build(self, out_ptr: int, chunks=None, nbranch: int = 4):
+        if chunks is None:
+            _check(lib.cintx_plan_graph_build(self.handle, None, 0, ctypes.c_void_p(out_ptr), nbranch))
+        else:
+            c = np.ascontiguousarray(chunks, dtype=np.int64)
+            _check(lib.cintx_plan_graph_build(self.handle, c.ctypes.data_as(_i64p), c.size,
+                                              ctypes.c_void_p(out_ptr), nbranch))
+
+    def graph_launch(self, stream: int = 0):
+        _check(lib.cintx_plan_graph_launch(self.handle, ctypes.c_void_p(stream)))
 
     def execute_host(self, out: np.ndarray, chunk: int = -1):
         assert out.dtype == np.float64 and out.flags.c_contiguous

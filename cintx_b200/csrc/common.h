@@ -38,6 +38,20 @@ struct __align__(16) QuartetRec {
   long long out;  // offset in doubles
 };
 
+// A contiguous run [t0, t1) of one screened tile's row-major quartet numbering, generating
+// records rec_off.. of a merged class segment whose blocks start at out_off (doubles).
+struct __align__(16) GenRange {
+  const int* rows;
+  const int* cols;
+  const long long* prefix;
+  int nrows;
+  int pad;
+  long long t0, t1;
+  long long rec_off;
+  long long out_off;
+  long long nout;
+};
+
 // Output placement of one launch group: the element (a, b, c, d) of the canonical block
 // (a over shell i components fastest) goes to out + rec.out + a*s0 + b*s1 + c*s2 + d*s3.
 struct OutStrides {

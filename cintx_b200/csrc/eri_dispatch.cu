@@ -21,4 +21,10 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
   return dispatch_eri(li, lj, lk, ll, sph, a);
 }
 
+bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph) {
+  LaunchArgs a{};
+  a.query = 1;
+  return dispatch_eri(li, lj, lk, ll, sph, a) == cudaErrorNotSupported;
+}
+
 }  // namespace cintx

@@ -17,6 +17,7 @@ struct LaunchArgs {
   RysTable rys;
   cudaStream_t stream;
   int max_blocks;  // grid cap (0: derived from the SM count)
+  int query = 0;   // 1: launch nothing; return cudaErrorNotSupported if the class needs scratch
 };
 
 // Device scratch for classes whose transform buffers live in global memory: returns a buffer
@@ -34,6 +35,7 @@ int device_sm_count();
 template <int LI, int LJ, int LK, int LL, bool SPH>
 cudaError_t launch_eri(const LaunchArgs& a) {
   using SH = EriShape<LI, LJ, LK, LL, SPH>;
+  if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
   auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH>;
   static int attr_done[64];
   int dev = 0;

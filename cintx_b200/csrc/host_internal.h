@@ -117,6 +117,7 @@ struct Oriented {
 double flops_per_prim_quartet(int li, int lj, int lk, int ll);
 double flops_c2s(int li, int lj, int lk, int ll, bool sph);
 
+bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph);
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream);

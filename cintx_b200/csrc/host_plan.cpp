@@ -24,6 +24,8 @@ namespace cintx {
 cudaError_t launch_gen_tile(const int* rows, const int* cols, const long long* row_prefix, int nrows,
                             long long t0, long long t1, long long nout, long long out_base, QuartetRec* recs,
                             cudaStream_t stream);
+cudaError_t launch_gen_ranges(const GenRange* ranges, int nranges, long long nrec, QuartetRec* recs,
+                              cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -44,10 +46,13 @@ struct Segment {
   long long nout = 0;      // doubles per block (screened)
   long long out_off = 0;   // chunk-relative output start of this segment
   double flops = 0;        // algorithmic FP64 flops of the segment
+  int range0 = 0;          // merged class segments (tile == -2): GenRange slice
+  int nranges = 0;
 };
 
 struct Chunk {
-  std::vector<Segment> segs;
+  std::vector<Segment> segs;     // execution units (one per kernel class for screened plans)
+  std::vector<Segment> pieces;   // screened: per-tile ranges in output order
   long long out_size = 0;
   long long nrec = 0;
 };
@@ -76,6 +81,13 @@ struct CintxPlan {
   std::vector<QuartetRec> h_recs;  // explicit plans keep a host copy for chunk_quartets
   std::vector<int> h_tuples;       // explicit: requested tuples (4 per record, -1 for unit)
   CintxPlanStats stats{};
+  std::vector<GenRange> ranges;    // screened: all merged-segment ranges
+  GenRange* d_ranges = nullptr;
+  // captured execution of a chunk list (cintx_plan_graph_build)
+  cudaGraphExec_t gexec = nullptr;
+  int64_t graph_kernels = 0;
+  std::vector<cudaStream_t> branches;
+  std::vector<cudaEvent_t> events;
   // end-to-end staging
   double* d_stage = nullptr;
   long long stage_cap = 0;
@@ -96,6 +108,14 @@ void free_plan_device(CintxPlan* p) {
   }
   if (p->d_stage) cudaFree(p->d_stage);
   p->d_stage = nullptr;
+  if (p->d_ranges) cudaFree(p->d_ranges);
+  p->d_ranges = nullptr;
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  p->gexec = nullptr;
+  for (cudaStream_t b : p->branches) cudaStreamDestroy(b);
+  p->branches.clear();
+  for (cudaEvent_t e : p->events) cudaEventDestroy(e);
+  p->events.clear();
   if (p->stream) cudaStreamDestroy(p->stream);
   p->stream = nullptr;
 }
@@ -307,7 +327,17 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
   const Opt* o = p->opt;
   const QuartetRec* recs;
   long long nrec;
-  if (sg.tile < 0) {
+  if (sg.tile == -2) {
+    QuartetRec* dst = p->d_recs + sg.rec0;
+    cudaError_t e = launch_gen_ranges(p->d_ranges + sg.range0, sg.nranges, sg.nrec, dst, stream);
+    if (e != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("quartet generation failed: ") + cudaGetErrorString(e));
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+    ts->launches++;
+    recs = dst;
+    nrec = sg.nrec;
+  } else if (sg.tile < 0) {
     recs = p->d_recs + sg.rec0;
     nrec = sg.nrec;
   } else {
@@ -440,7 +470,7 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
   const Chunk& ch = p->chunks[chunk];
   const Opt* o = p->opt;
   int64_t k = 0;
-  for (const Segment& sg : ch.segs) {
+  for (const Segment& sg : (ch.pieces.empty() ? ch.segs : ch.pieces)) {
     if (sg.tile < 0) {
       // explicit plans list tuples per record (group order), as requested
       for (long long r = 0; r < sg.nrec; ++r, ++k) {
@@ -476,7 +506,7 @@ int cintx_plan_chunk_segments(const CintxPlan* p, int64_t chunk, int* cls, int64
       cls[4 * s + 2] = sg.lk;
       cls[4 * s + 3] = sg.ll;
     }
-    if (nq) nq[s] = sg.tile < 0 ? sg.nrec : sg.t1 - sg.t0;
+    if (nq) nq[s] = sg.tile < 0 ? sg.nrec : sg.t1 - sg.t0;  // merged (-2) and explicit (-1) use nrec
     if (flops) flops[s] = sg.flops;
   }
   return n;
@@ -518,6 +548,119 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
       for (int a = 0; a < 4; ++a) quartets[k * 4 + a] = p->h_tuples[g * 4 + a];
     }
   }
+  return CINTX_STATUS_SUCCESS;
+}
+
+// Captures the execution of `chunks` (n entries; all when chunks == NULL) into one CUDA graph
+// writing to out_dev.  Inside a chunk the kernel classes are independent (disjoint outputs)
+// and are spread over `nbranch` parallel branches by their flop estimate; chunks follow each
+// other because they share out_dev.
+int cintx_plan_graph_build(CintxPlan* p, const int64_t* chunks, int64_t n, double* out_dev, int nbranch) {
+  clear_error();
+  if (!p || !out_dev) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and out_dev must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  std::vector<int64_t> list;
+  if (chunks) list.assign(chunks, chunks + n);
+  else
+    for (int64_t c = 0; c < (int64_t)p->chunks.size(); ++c) list.push_back(c);
+  for (int64_t c : list) {
+    if (c < 0 || c >= (int64_t)p->chunks.size()) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "chunk index out of range");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+    for (const Segment& sg : p->chunks[c].segs)
+      if (class_needs_scratch(sg.li, sg.lj, sg.lk, sg.ll, p->sph)) {
+        set_error(CINTX_STATUS_UNSUPPORTED_API, "plan contains classes with device scratch; use cintx_plan_execute");
+        return CINTX_STATUS_UNSUPPORTED_API;
+      }
+  }
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc;
+  if ((rc = device_state(&ds)) || (rc = thread_scratch(&ts, 0, 0))) return rc;
+  nbranch = std::max(1, std::min(nbranch, 16));
+  if (p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  while ((int)p->branches.size() < nbranch) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+    p->branches.push_back(s);
+  }
+  while ((int)p->events.size() < nbranch + 1) {
+    cudaEvent_t e;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    p->events.push_back(e);
+  }
+  cudaStream_t origin = p->branches[0];
+  if (cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "stream capture could not start");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  const int64_t l0 = ts->launches;
+  for (int64_t c : list) {
+    const Chunk& ch = p->chunks[c];
+    cudaEventRecord(p->events[0], origin);
+    for (int b = 1; b < nbranch; ++b) cudaStreamWaitEvent(p->branches[b], p->events[0], 0);
+    // longest-first assignment of class segments to branches
+    std::vector<int> idx(ch.segs.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return ch.segs[a].flops > ch.segs[b].flops; });
+    std::vector<double> load(nbranch, 0.0);
+    for (int i : idx) {
+      const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[b] += ch.segs[i].flops + 1.0;
+      if ((rc = run_segment(p, ch.segs[i], out_dev, p->branches[b], ds, ts))) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(origin, &g);
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+    }
+    for (int b = 1; b < nbranch; ++b) {
+      cudaEventRecord(p->events[b], p->branches[b]);
+      cudaStreamWaitEvent(origin, p->events[b], 0);
+    }
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(origin, &graph);
+  if (e != cudaSuccess || !graph) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("stream capture failed: ") + cudaGetErrorString(e));
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  e = cudaGraphInstantiate(&p->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    p->gexec = nullptr;
+    set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  p->graph_kernels = ts->launches - l0;
+  ts->launches = l0;  // captured, not launched
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_graph_launch(CintxPlan* p, void* stream) {
+  clear_error();
+  if (!p || !p->gexec) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "plan has no captured graph");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  ThreadScratch* ts;
+  int rc;
+  if ((rc = thread_scratch(&ts, 0, 0))) return rc;
+  cudaError_t e = cudaGraphLaunch(p->gexec, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("graph launch failed: ") + cudaGetErrorString(e));
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  ts->launches += p->graph_kernels;
   return CINTX_STATUS_SUCCESS;
 }
 
@@ -669,7 +812,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
     while (q < nq) {
       long long room = (max_chunk - cur.out_size) / nout;
       if (room <= 0) {
-        if (cur.segs.empty()) room = 1;  // a single block larger than the chunk limit
+        if (cur.pieces.empty()) room = 1;  // a single block larger than the chunk limit
         else {
           p->chunks.push_back(cur);
           max_recs = std::max(max_recs, cur.nrec);
@@ -706,13 +849,13 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
         }
         sg.flops = fl + take * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
       }
-      cur.segs.push_back(sg);
+      cur.pieces.push_back(sg);
       cur.nrec += take;
       cur.out_size += take * nout;
       q += take;
     }
   }
-  if (!cur.segs.empty()) {
+  if (!cur.pieces.empty()) {
     p->chunks.push_back(cur);
     max_recs = std::max(max_recs, cur.nrec);
   }
@@ -730,6 +873,65 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
       cudaMemcpy(t.d_prefix, t.row_prefix.data(), sizeof(long long) * t.row_prefix.size(), cudaMemcpyHostToDevice);
     }
+  }
+  // merge each chunk's tile pieces into one segment per kernel class (records of a class are
+  // contiguous; each record carries its chunk-relative output offset)
+  for (Chunk& ch : p->chunks) {
+    std::vector<int> order;
+    std::map<std::tuple<int, int, int, int>, int> first;
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < (int)ch.pieces.size(); ++i) {
+      const Segment& pc = ch.pieces[i];
+      auto key = std::make_tuple(pc.li, pc.lj, pc.lk, pc.ll);
+      auto it = first.find(key);
+      if (it == first.end()) {
+        first[key] = (int)members.size();
+        members.push_back({i});
+      } else {
+        members[it->second].push_back(i);
+      }
+    }
+    ch.segs.clear();
+    long long rec = 0;
+    for (auto& mem : members) {
+      const Segment& p0 = ch.pieces[mem[0]];
+      Segment m;
+      m.li = p0.li;
+      m.lj = p0.lj;
+      m.lk = p0.lk;
+      m.ll = p0.ll;
+      m.st = p0.st;
+      m.expcutoff = p0.expcutoff;
+      m.tile = -2;
+      m.rec0 = rec;
+      m.out_off = 0;
+      m.range0 = (int)p->ranges.size();
+      for (int i : mem) {
+        const Segment& pc = ch.pieces[i];
+        const Tile& t = p->tiles[pc.tile];
+        GenRange g;
+        g.rows = t.d_rows;
+        g.cols = t.d_cols;
+        g.prefix = t.d_prefix;
+        g.nrows = (int)t.rows.size();
+        g.pad = 0;
+        g.t0 = pc.t0;
+        g.t1 = pc.t1;
+        g.rec_off = m.nrec;
+        g.out_off = pc.out_off;
+        g.nout = pc.nout;
+        p->ranges.push_back(g);
+        m.nrec += pc.t1 - pc.t0;
+        m.flops += pc.flops;
+      }
+      m.nranges = (int)p->ranges.size() - m.range0;
+      rec += m.nrec;
+      ch.segs.push_back(m);
+    }
+  }
+  if (ok && !p->ranges.empty()) {
+    ok = cudaMalloc(&p->d_ranges, sizeof(GenRange) * p->ranges.size()) == cudaSuccess;
+    if (ok) cudaMemcpy(p->d_ranges, p->ranges.data(), sizeof(GenRange) * p->ranges.size(), cudaMemcpyHostToDevice);
   }
   if (!ok) {
     free_plan_device(p);

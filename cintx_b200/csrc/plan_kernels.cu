@@ -41,3 +41,43 @@ cudaError_t launch_gen_tile(const int* rows, const int* cols, const long long* r
   return cudaGetLastError();
 }
 }  // namespace cintx
+
+// Multi-range generation: one launch fills the records of every tile range of a kernel class
+// within a chunk.  ranges[] are ordered by rec_off; record r belongs to the last range whose
+// rec_off <= r.
+__global__ void gen_range_quartets(const GenRange* __restrict__ ranges, int nranges, long long nrec,
+                                   QuartetRec* __restrict__ recs) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nrec;
+       r += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nranges - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ranges[mid].rec_off <= r) lo = mid;
+      else hi = mid - 1;
+    }
+    const GenRange g = ranges[lo];
+    const long long t = g.t0 + (r - g.rec_off);
+    int a = 0, b = g.nrows - 1;
+    while (a < b) {
+      const int mid = (a + b + 1) >> 1;
+      if (g.prefix[mid] <= t) a = mid;
+      else b = mid - 1;
+    }
+    QuartetRec q;
+    q.pij = g.rows[a];
+    q.pkl = g.cols[t - g.prefix[a]];
+    q.out = g.out_off + (r - g.rec_off) * g.nout;
+    recs[r] = q;
+  }
+}
+
+namespace cintx {
+cudaError_t launch_gen_ranges(const GenRange* ranges, int nranges, long long nrec, QuartetRec* recs,
+                              cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec + 255) / 256;
+  if (blocks > 65535) blocks = 65535;
+  gen_range_quartets<<<(unsigned)blocks, 256, 0, stream>>>(ranges, nranges, nrec, recs);
+  return cudaGetLastError();
+}
+}  // namespace cintx

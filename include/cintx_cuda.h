@@ -159,6 +159,13 @@ CINTX_API int cintx_plan_sample_quartets(const CintxPlan *plan, uint64_t seed, i
  * (a cudaStream_t; NULL = the library's per-thread stream).  out_dev is device memory of
  * at least the chunk size (all-chunk runs: max_chunk_doubles).  Asynchronous. */
 CINTX_API int cintx_plan_execute(CintxPlan *plan, int64_t chunk, double *out_dev, void *stream);
+/* Captures the execution of a chunk list (chunks == NULL: every chunk) into one CUDA graph
+ * writing to out_dev: within a chunk the kernel classes run on up to nbranch parallel graph
+ * branches; chunks run in order.  Replaces any previous capture of this plan. */
+CINTX_API int cintx_plan_graph_build(CintxPlan *plan, const int64_t *chunks, int64_t n, double *out_dev,
+                                     int nbranch);
+/* Launches the captured graph on `stream` (asynchronous). */
+CINTX_API int cintx_plan_graph_launch(CintxPlan *plan, void *stream);
 /* Same, end to end: device output staged through a device ring and copied to host memory
  * out_host (at least chunk size; all-chunk runs overwrite it per chunk).  Synchronous. */
 CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);

@@ -170,6 +170,26 @@ def test_screened_plan_mol40(cx, orc):
         plan.close()
 
 
+def test_graph_replay_matches_direct_execution(cx):
+    mol = M.mol40()
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 25)
+        st = plan.stats
+        a = torch.zeros(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        b = torch.zeros_like(a)
+        s = torch.cuda.current_stream().cuda_stream
+        last = st.nchunks - 1
+        plan.execute(a.data_ptr(), chunk=last, stream=s)
+        plan.graph_build(b.data_ptr(), chunks=[last], nbranch=4)
+        plan.graph_launch(s)
+        plan.graph_launch(s)
+        torch.cuda.synchronize()
+        n = plan.chunk_size(last)
+        assert torch.equal(a[:n], b[:n])
+        plan.close()
+
+
 def orc_block(mol, q):
     n = 1
     for s in q:
