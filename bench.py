@@ -286,7 +286,8 @@ def our_arm(args):
     owner = balance(chunk_flops, world)
     mine = [c for c in range(nchunks) if owner[c] == rank]
     my_ints = sum(plan.chunk_size(c) for c in mine)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
+    torch.cuda.set_stream(stream)
     ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 

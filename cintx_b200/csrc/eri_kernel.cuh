@@ -82,6 +82,9 @@ struct EriShape {
       S == 1 ? 0 : cmax(SM_ROOTS + SM_G + SM_SCR, GLOBAL_BUF ? 0 : SM_BUFA + SM_BUFB);
   static constexpr int SM_GROUP = (SM_GROUP_RAW + 1) & ~1;  // 16-byte multiple
   static constexpr int BLOCK = S >= 128 ? S : 128;
+  // resident blocks requested from the register allocator: <= 128 registers per thread for the
+  // multi-lane kernels (their stalls are latency bound and need warps)
+  static constexpr int MINB = S == 1 ? 1 : 65536 / (BLOCK * 128);
   static constexpr int Q = BLOCK / S;
   static constexpr int SMEM_BYTES = Q * SM_GROUP * 8;
 };
@@ -244,8 +247,81 @@ __device__ __forceinline__ void decode_tuples(LaneTuples<SH>& lt, int lane) {
   }
 }
 
+// Primitive loop of the one-lane classes: U primitive quartets per iteration as independent
+// chains (their pair loads, root-table loads and recurrences overlap), accumulated into the
+// lane's cartesian block.  Slots past the end or screened out contribute with a zero factor.
+template <int LI, int LJ, int LK, int LL, int U, class SH>
+__device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const ShellPair& pkl,
+                                                   const PrimPair* __restrict__ prims, const RysTable& rys,
+                                                   double expcutoff, const LaneTuples<SH>& lt,
+                                                   double (&acc)[SH::TPT][SH::NFI]) {
+  constexpr int NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
+  const int nij = pij.nprim, ntot = nij * pkl.nprim;
+  int ia[U], ib[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    ib[u] = u / nij;
+    ia[u] = u - ib[u] * nij;
+  }
+  for (int base = 0; base < ntot; base += U) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool valid = base + u < ntot;
+      const PrimPair pi = prims[pij.prim_off + (valid ? ia[u] : 0)];
+      const PrimPair pk = prims[pkl.prim_off + (valid ? ib[u] : 0)];
+      // CINT2e_loop eijcutoff screening (cint2e.c:700-712)
+      const bool keep = valid && !(pi.cce + pk.cce > expcutoff);
+      const double aij = pi.aij, akl = pk.aij;
+      const double aijkl = aij + akl;
+      const double rs = rsqrt(aijkl);
+      const double inv_aijkl = rs * rs;
+      const double a1 = aij * akl;
+      const double inv_a1 = 4.0 * pi.half_inv * pk.half_inv;
+      const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
+      const double rr = pqx * pqx + pqy * pqy + pqz * pqz;
+      const double x = keep ? a1 * inv_aijkl * rr : 0.0;
+      const double fac = keep ? pi.kab * pk.kab * rs * inv_a1 : 0.0;
+      double t2[NR], w[NR];
+      if constexpr (LI + LJ + LK + LL == 0) {
+        rys_all<NR, NR, 2 * NR>(rys, x, t2, w);  // (ss|ss) needs the weight only
+        acc[0][0] = fma(w[0], fac, acc[0][0]);
+      } else {
+        rys_all<NR>(rys, x, t2, w);
+        const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
+        const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          double gg[3 * GSZ];
+          const double rt_aa = t2[r] * inv_aijkl;
+          const double b00 = 0.5 * rt_aa;
+          const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
+          const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
+          const double ca = rt_aa * akl, cb = rt_aa * aij;
+          vrr_hrr<LI, LJ, LK, LL>(gg + 0 * GSZ, 1.0, pax - ca * pqx, qcx + cb * pqx, b10, b01, b00, pij.abx, pkl.abx);
+          vrr_hrr<LI, LJ, LK, LL>(gg + 1 * GSZ, 1.0, pay - ca * pqy, qcy + cb * pqy, b10, b01, b00, pij.aby, pkl.aby);
+          vrr_hrr<LI, LJ, LK, LL>(gg + 2 * GSZ, w[r] * fac, paz - ca * pqz, qcz + cb * pqz, b10, b01, b00, pij.abz,
+                                  pkl.abz);
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+            for (int fi = 0; fi < NFI; ++fi) {
+              acc[k][fi] = fma(gg[cart_x(LI, fi) + lt.ox[k]] * gg[GSZ + cart_y(LI, fi) + lt.oy[k]],
+                               gg[2 * GSZ + cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
+            }
+          }
+        }
+      }
+      ia[u] += U;
+      while (ia[u] >= nij) {
+        ia[u] -= nij;
+        ++ib[u];
+      }
+    }
+  }
+}
+
 template <int LI, int LJ, int LK, int LL, bool SPH>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK)
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape<LI, LJ, LK, LL, SPH>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch) {
@@ -276,6 +352,11 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK)
 #pragma unroll
       for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
 
+    if constexpr (S == 1) {
+      constexpr int U = (LI + LJ + LK + LL == 0) ? 4 : 2;
+      if (pij.nprim * pkl.nprim >= U) prim_loop_one_lane<LI, LJ, LK, LL, U, SH>(pij, pkl, prims, rys, expcutoff, lt, acc);
+      else prim_loop_one_lane<LI, LJ, LK, LL, 1, SH>(pij, pkl, prims, rys, expcutoff, lt, acc);
+    } else
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];
       const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
@@ -345,7 +426,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK)
           group_sync<S>(group);
         }
         // cartesian products, summed over roots
-#pragma unroll(SH::NR * SH::TPT * SH::NFI <= 256 ? SH::NR : 1)
+#pragma unroll 1
         for (int r = 0; r < NR; ++r) {
           const double* gx = gg + (0 * NR + r) * GSZ;
           const double* gy = gg + (1 * NR + r) * GSZ;

@@ -376,7 +376,7 @@ static int exec_prepare(CintxPlan* p, double* out_dev, void* stream_, cudaStream
   int rc;
   if ((rc = device_state(ds))) return rc;
   if ((rc = thread_scratch(ts, 0, 0))) return rc;
-  *stream = stream_ ? (cudaStream_t)stream_ : (*ts)->stream;
+  *stream = (cudaStream_t)stream_;  // used as given: 0 is the legacy default stream
   return CINTX_STATUS_SUCCESS;
 }
 

@@ -10,6 +10,24 @@
 #pragma once
 #include "common.h"
 
+// Device layout (transposed from the file at upload): per order n, interval i, function f the
+// DEG+1 monomial coefficients are contiguous (16-byte aligned), so one function costs
+// (DEG+1)/2 vector loads.
+constexpr int RYS_NC = CINTX_RYS_DEG + 1;  // coefficients per function (even)
+
+__device__ __forceinline__ double rys_horner(const double* __restrict__ c, double z) {
+  const double2* c2 = reinterpret_cast<const double2*>(c);
+  const double2 hi = __ldg(c2 + RYS_NC / 2 - 1);
+  double acc = fma(hi.y, z, hi.x);
+#pragma unroll
+  for (int k = RYS_NC / 2 - 2; k >= 0; --k) {
+    const double2 v = __ldg(c2 + k);
+    acc = fma(acc, z, v.y);
+    acc = fma(acc, z, v.x);
+  }
+  return acc;
+}
+
 // Function f of order n at x: f < n -> t^2 of root f, else weight of root f - n.
 __device__ __forceinline__ double rys_fn(const RysTable& c_rys, int n, int f, double x) {
   const int xmax = c_rys.xmax[n];
@@ -19,42 +37,31 @@ __device__ __forceinline__ double rys_fn(const RysTable& c_rys, int n, int f, do
   }
   const int i = (int)x;
   const double z = 2.0 * (x - (double)i) - 1.0;
-  const double* c = c_rys.poly[n] + (size_t)i * (CINTX_RYS_DEG + 1) * 2 * n + f;
-  double acc = __ldg(c + CINTX_RYS_DEG * 2 * n);
-#pragma unroll
-  for (int k = CINTX_RYS_DEG - 1; k >= 0; --k) acc = fma(acc, z, __ldg(c + k * 2 * n));
-  return acc;
+  return rys_horner(c_rys.poly[n] + ((size_t)i * 2 * n + f) * RYS_NC, z);
 }
 
-// All 2n functions at once (one thread).  Coefficient rows are contiguous per degree.
-template <int N>
+// Functions [F0, F1) of order N at once (one thread); F0 = N, F1 = 2N gives the weights only.
+template <int N, int F0 = 0, int F1 = 2 * N>
 __device__ __forceinline__ void rys_all(const RysTable& c_rys, double x, double* t2, double* w) {
   const int xmax = c_rys.xmax[N];
   if (!(x < (double)xmax)) {  // also routes NaN away from the table index
     const double* a = c_rys.asym[N];
-    const double inv = 1.0 / x;
     const double rs = rsqrt(x);
+    const double inv = rs * rs;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      t2[r] = __ldg(a + r) * inv;
+      if (F0 <= r) t2[r] = __ldg(a + r) * inv;
       w[r] = __ldg(a + N + r) * rs;
     }
     return;
   }
   const int i = (int)x;
   const double z = 2.0 * (x - (double)i) - 1.0;
-  const double* c = c_rys.poly[N] + (size_t)i * (CINTX_RYS_DEG + 1) * 2 * N;
-  double acc[2 * N];
+  const double* c = c_rys.poly[N] + (size_t)i * 2 * N * RYS_NC;
 #pragma unroll
-  for (int f = 0; f < 2 * N; ++f) acc[f] = __ldg(c + CINTX_RYS_DEG * 2 * N + f);
-#pragma unroll
-  for (int k = CINTX_RYS_DEG - 1; k >= 0; --k) {
-#pragma unroll
-    for (int f = 0; f < 2 * N; ++f) acc[f] = fma(acc[f], z, __ldg(c + k * 2 * N + f));
-  }
-#pragma unroll
-  for (int r = 0; r < N; ++r) {
-    t2[r] = acc[r];
-    w[r] = acc[N + r];
+  for (int f = F0; f < F1; ++f) {
+    const double v = rys_horner(c + f * RYS_NC, z);
+    if (f < N) t2[f] = v;
+    else w[f - N] = v;
   }
 }

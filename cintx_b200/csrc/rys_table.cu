@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
+
+#include <vector>
 #include "common.h"
 
 extern "C" const unsigned char cintx_rys_table_bin[];
@@ -26,10 +28,28 @@ int upload_rys_table(void** dev_buf, RysTable* tab) {
   int64_t hdr[16];
   memcpy(hdr, p, sizeof(hdr));
   const int nmax = (int)hdr[0], deg = (int)hdr[1];
-  if (nmax < CINTX_NRMAX || deg != CINTX_RYS_DEG) return 1;
+  if (nmax < CINTX_NRMAX || deg != CINTX_RYS_DEG || (deg + 1) % 2) return 1;
+  // transpose every interval from [degree][function] (file) to [function][degree] (device)
+  std::vector<double> host((nbytes - sizeof(hdr)) / sizeof(double));
+  memcpy(host.data(), p + sizeof(hdr), nbytes - sizeof(hdr));
+  {
+    size_t o = 0;
+    std::vector<double> tmp;
+    for (int n = 1; n <= nmax; ++n) {
+      const int nf = 2 * n, nc = deg + 1;
+      const int xmax = (int)hdr[1 + n];
+      for (int i = 0; i < xmax; ++i, o += (size_t)nf * nc) {
+        tmp.assign(host.begin() + o, host.begin() + o + (size_t)nf * nc);
+        for (int k = 0; k < nc; ++k)
+          for (int f = 0; f < nf; ++f) host[o + (size_t)f * nc + k] = tmp[(size_t)k * nf + f];
+      }
+    }
+  }
   void* d = nullptr;
   if (cudaMalloc(&d, nbytes) != cudaSuccess) return 2;
-  if (cudaMemcpy(d, p, nbytes, cudaMemcpyHostToDevice) != cudaSuccess) return 3;
+  if (cudaMemcpy(d, p, sizeof(hdr), cudaMemcpyHostToDevice) != cudaSuccess) return 3;
+  if (cudaMemcpy((char*)d + sizeof(hdr), host.data(), nbytes - sizeof(hdr), cudaMemcpyHostToDevice) != cudaSuccess)
+    return 3;
   RysTable t;
   memset(&t, 0, sizeof(t));
   const double* base = (const double*)((const char*)d + sizeof(hdr));

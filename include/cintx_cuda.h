@@ -156,7 +156,7 @@ CINTX_API int cintx_plan_execute_segment(CintxPlan *plan, int64_t chunk, int seg
 CINTX_API int cintx_plan_sample_quartets(const CintxPlan *plan, uint64_t seed, int64_t n, int *quartets);
 
 /* Run one chunk (or all chunks when chunk < 0, each overwriting out_dev) on `stream`
- * (a cudaStream_t; NULL = the library's per-thread stream).  out_dev is device memory of
+ * (a cudaStream_t, used as given: NULL is the legacy default stream).  out_dev is device memory of
  * at least the chunk size (all-chunk runs: max_chunk_doubles).  Asynchronous. */
 CINTX_API int cintx_plan_execute(CintxPlan *plan, int64_t chunk, double *out_dev, void *stream);
 /* Captures the execution of a chunk list (chunks == NULL: every chunk) into one CUDA graph
