@@ -171,6 +171,32 @@ CINTX_API int cintx_plan_graph_launch(CintxPlan *plan, void *stream);
 CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);
 CINTX_API void cintx_plan_destroy(CintxPlan *plan);
 
+/* ---- evaluation without device allocation ------------------------------------------------ */
+
+/* Size of the fixed device scratch array behind cintx_int2e_noalloc (32 MiB per GPU). */
+#define CINTX_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* Has no counterpart in the reference; it exists for callers that cannot call cudaMalloc while
+ * they use this library: code running inside a host framework's memory pool or arena, code that
+ * has already claimed almost all HBM, and code that must avoid the device-wide synchronisation an
+ * allocation or free may cause.  Evaluates int2e (sph != 0: spherical, else cartesian) for n
+ * shell quartets (shls: 4 ints each, host) of the basis (atm, bas, env: host arrays as for
+ * int2e_sph) into out_dev, device memory the caller owns, with the blocks back to back in list
+ * order in libcint's dims == NULL layout (the offsets cintx_plan_shells reports).  It calls no
+ * cudaMalloc/cudaFree: its device working memory is a static array of
+ * CINTX_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the process exits,
+ * plus a static copy of the root table.  The first call on each device does a one-time set-up
+ * (looks up the arrays' device addresses and copies the root table, synchronously); make that
+ * first call before any stream capture.  A call whose screened pairs and quartet records exceed
+ * the array returns CINTX_STATUS_MEMORY_LIMIT_EXCEEDED (split the list); classes with two or
+ * more g shells return CINTX_STATUS_UNSUPPORTED_API.  Work is queued on `stream` (used as
+ * given) and the function returns once its inputs have been copied.  Every call reuses the
+ * same array and rewrites all of it that it reads, so nothing needs clearing between calls, but
+ * calls whose work overlaps on the GPU (other streams, other host threads) race on it:
+ * serialise them. */
+CINTX_API int cintx_int2e_noalloc(double *out_dev, const int *shls, int64_t n, int sph, const int *atm,
+                                  int natm, const int *bas, int nbas, const double *env, void *stream);
+
 /* FP64 FMA throughput probe (measurement only): blocks x threads threads each run
  * iters*16*8 FMAs and write one double to out_dev[blocks*threads].  Asynchronous on stream. */
 CINTX_API int cintx_fp64_fma_probe(int blocks, int threads, int iters, double *out_dev, void *stream);
