@@ -10,6 +10,12 @@
 #define CINTX_NRMAX 9         // highest Rys order: (4+4+4+4)/2 + 1
 #define CINTX_RYS_DEG 11      // polynomial degree per unit-width x interval
 
+// Table intervals per order (x < xmax uses the table; the file header must match).
+__host__ __device__ constexpr int cintx_rys_xmax(int n) {
+  return n == 1 ? 40 : n == 2 ? 52 : n == 3 ? 60 : n == 4 ? 64 : n == 5 ? 72 : n == 6 ? 76 : n == 7 ? 84
+       : n == 8 ? 92 : 100;
+}
+
 // One primitive pair (a, b) of an oriented shell pair (i, j), after exponent screening.
 // kab folds exp(-a_i a_j/a_ij |A-B|^2), both contraction coefficients (single contraction)
 // and the pair's share of libcint's common factor sqrt(2 pi^2.5) * fac_sp(li) * fac_sp(lj).

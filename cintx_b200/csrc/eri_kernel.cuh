@@ -86,7 +86,11 @@ struct EriShape {
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : 65536 / (BLOCK * 128);
   static constexpr int Q = BLOCK / S;
-  static constexpr int SMEM_BYTES = Q * SM_GROUP * 8;
+  // one-lane classes of low order stage their root-table block in shared memory: the lanes'
+  // scattered coefficient loads then cost shared-memory wavefronts instead of L1 sectors
+  static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
+  static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
+  static constexpr int SMEM_BYTES = Q * SM_GROUP * 8 + TABLE_DOUBLES * 8;
 };
 
 // Group barrier: warp-level for S <= 32, a named barrier per group above.
@@ -247,30 +251,23 @@ __device__ __forceinline__ void decode_tuples(LaneTuples<SH>& lt, int lane) {
   }
 }
 
-// Primitive loop of the one-lane classes: U primitive quartets per iteration as independent
-// chains (their pair loads, root-table loads and recurrences overlap), accumulated into the
-// lane's cartesian block.  Slots past the end or screened out contribute with a zero factor.
-template <int LI, int LJ, int LK, int LL, int U, class SH>
+// Primitive loop of the one-lane classes.  Quartets of a warp share their (ij) pair (row-major
+// tiles), so the inner loop's primitive-pair loads are warp-wide broadcasts; the lane's (kl)
+// primitive pair is loaded once per outer iteration.  `tab` is the shared-memory copy of the
+// order-NR root table when SH::STAGE_TABLE (otherwise the global table is read).
+template <int LI, int LJ, int LK, int LL, class SH>
 __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const ShellPair& pkl,
                                                    const PrimPair* __restrict__ prims, const RysTable& rys,
-                                                   double expcutoff, const LaneTuples<SH>& lt,
+                                                   const double* tab, double expcutoff, const LaneTuples<SH>& lt,
                                                    double (&acc)[SH::TPT][SH::NFI]) {
   constexpr int NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
-  const int nij = pij.nprim, ntot = nij * pkl.nprim;
-  int ia[U], ib[U];
-#pragma unroll
-  for (int u = 0; u < U; ++u) {
-    ib[u] = u / nij;
-    ia[u] = u - ib[u] * nij;
-  }
-  for (int base = 0; base < ntot; base += U) {
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const bool valid = base + u < ntot;
-      const PrimPair pi = prims[pij.prim_off + (valid ? ia[u] : 0)];
-      const PrimPair pk = prims[pkl.prim_off + (valid ? ib[u] : 0)];
-      // CINT2e_loop eijcutoff screening (cint2e.c:700-712)
-      const bool keep = valid && !(pi.cce + pk.cce > expcutoff);
+  constexpr bool SSSS = LI + LJ + LK + LL == 0;
+  for (int b = 0; b < pkl.nprim; ++b) {
+    const PrimPair pk = prims[pkl.prim_off + b];
+    const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+    for (int a = 0; a < pij.nprim; ++a) {
+      const PrimPair pi = prims[pij.prim_off + a];
+      if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
       const double aij = pi.aij, akl = pk.aij;
       const double aijkl = aij + akl;
       const double rs = rsqrt(aijkl);
@@ -279,16 +276,20 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
       const double inv_a1 = 4.0 * pi.half_inv * pk.half_inv;
       const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
       const double rr = pqx * pqx + pqy * pqy + pqz * pqz;
-      const double x = keep ? a1 * inv_aijkl * rr : 0.0;
-      const double fac = keep ? pi.kab * pk.kab * rs * inv_a1 : 0.0;
+      const double x = a1 * inv_aijkl * rr;
+      const double fac = pi.kab * pk.kab * rs * inv_a1;
       double t2[NR], w[NR];
-      if constexpr (LI + LJ + LK + LL == 0) {
-        rys_all<NR, NR, 2 * NR>(rys, x, t2, w);  // (ss|ss) needs the weight only
-        acc[0][0] = fma(w[0], fac, acc[0][0]);
+      if constexpr (SH::STAGE_TABLE) {
+        if constexpr (SSSS) rys_all_staged<NR, NR, 2 * NR>(tab, rys, x, t2, w);
+        else rys_all_staged<NR>(tab, rys, x, t2, w);
       } else {
-        rys_all<NR>(rys, x, t2, w);
+        if constexpr (SSSS) rys_all<NR, NR, 2 * NR>(rys, x, t2, w);
+        else rys_all<NR>(rys, x, t2, w);
+      }
+      if constexpr (SSSS) {
+        acc[0][0] = fma(w[0], fac, acc[0][0]);  // (ss|ss) needs the weight only
+      } else {
         const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
-        const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
           double gg[3 * GSZ];
@@ -311,11 +312,6 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
           }
         }
       }
-      ia[u] += U;
-      while (ia[u] >= nij) {
-        ia[u] -= nij;
-        ++ib[u];
-      }
     }
   }
 }
@@ -335,6 +331,13 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
   double* s_g = sg + SH::SM_ROOTS;      // [axis][root][GSZ]
   double* s_scr = s_g + SH::SM_G;       // per-lane 2D tables (lanes < 3*NR)
 
+  if constexpr (SH::STAGE_TABLE) {
+    const double2* src = reinterpret_cast<const double2*>(rys.poly[NR]);
+    double2* dst = reinterpret_cast<double2*>(smem);
+    for (int i = threadIdx.x; i < SH::TABLE_DOUBLES / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+  }
+
   LaneTuples<SH> lt;
   decode_tuples<SH, LJ, LK, LL>(lt, lane);
 
@@ -353,9 +356,8 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
       for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
 
     if constexpr (S == 1) {
-      constexpr int U = (LI + LJ + LK + LL == 0) ? 4 : 2;
-      if (pij.nprim * pkl.nprim >= U) prim_loop_one_lane<LI, LJ, LK, LL, U, SH>(pij, pkl, prims, rys, expcutoff, lt, acc);
-      else prim_loop_one_lane<LI, LJ, LK, LL, 1, SH>(pij, pkl, prims, rys, expcutoff, lt, acc);
+      prim_loop_one_lane<LI, LJ, LK, LL, SH>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff, lt,
+                                             acc);
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];

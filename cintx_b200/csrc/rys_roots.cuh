@@ -65,3 +65,39 @@ __device__ __forceinline__ void rys_all(const RysTable& c_rys, double x, double*
     else w[f - N] = v;
   }
 }
+
+// As rys_all, with the order-N coefficient block (cintx_rys_xmax(N) intervals) staged in shared
+// memory at `tab`; only the large-x limit reads global memory.
+template <int N, int F0 = 0, int F1 = 2 * N>
+__device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable& c_rys, double x, double* t2,
+                                               double* w) {
+  constexpr int xmax = cintx_rys_xmax(N);
+  if (!(x < (double)xmax)) {  // also routes NaN away from the table index
+    const double* a = c_rys.asym[N];
+    const double rs = rsqrt(x);
+    const double inv = rs * rs;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      if (F0 <= r) t2[r] = __ldg(a + r) * inv;
+      w[r] = __ldg(a + N + r) * rs;
+    }
+    return;
+  }
+  const int i = (int)x;
+  const double z = 2.0 * (x - (double)i) - 1.0;
+  const double* c = tab + (size_t)i * 2 * N * RYS_NC;
+#pragma unroll
+  for (int f = F0; f < F1; ++f) {
+    const double2* c2 = reinterpret_cast<const double2*>(c + f * RYS_NC);
+    const double2 hi = c2[RYS_NC / 2 - 1];
+    double acc = fma(hi.y, z, hi.x);
+#pragma unroll
+    for (int k = RYS_NC / 2 - 2; k >= 0; --k) {
+      const double2 v = c2[k];
+      acc = fma(acc, z, v.y);
+      acc = fma(acc, z, v.x);
+    }
+    if (f < N) t2[f] = acc;
+    else w[f - N] = acc;
+  }
+}

@@ -56,6 +56,7 @@ int upload_rys_table(void** dev_buf, RysTable* tab) {
   size_t off = 0;
   for (int n = 1; n <= nmax; ++n) {
     int xmax = (int)hdr[1 + n];
+    if (n <= CINTX_NRMAX && xmax != cintx_rys_xmax(n)) return 6;
     if (n <= CINTX_NRMAX) {
       t.poly[n] = base + off;
       t.xmax[n] = xmax;
