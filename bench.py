@@ -37,6 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from cintx_b200 import molecules as M  # noqa: E402
+from cintx_b200.sharding import assign_chunks, chunks_of, max_over_ranks  # noqa: E402
 
 WORKLOADS = {
     "mol40_spd": (M.mol40, "40 seeded atoms in a 14-bohr cube, 60% light (2s,1p) / 40% heavy "
@@ -250,18 +251,6 @@ def fp64_peak(cx, torch):
     return best
 
 
-def balance(costs, nranks):
-    """Greedy longest-processing-time assignment of chunks to ranks."""
-    order = sorted(range(len(costs)), key=lambda c: -costs[c])
-    load = [0.0] * nranks
-    owner = [0] * len(costs)
-    for c in order:
-        r = min(range(nranks), key=lambda k: load[k])
-        owner[c] = r
-        load[r] += costs[c]
-    return owner
-
-
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -283,8 +272,8 @@ def our_arm(args):
     nchunks = st.nchunks
     seg_info = [plan.segments(c) for c in range(nchunks)]
     chunk_flops = [float(s[2].sum()) for s in seg_info]
-    owner = balance(chunk_flops, world)
-    mine = [c for c in range(nchunks) if owner[c] == rank]
+    owner = assign_chunks(chunk_flops, world)
+    mine = chunks_of(owner, rank)
     my_ints = sum(plan.chunk_size(c) for c in mine)
     stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
     torch.cuda.set_stream(stream)
@@ -330,11 +319,7 @@ def our_arm(args):
     t_wall = time.perf_counter() - t_wall
     launches = cx.launch_count() - launches0
     clk = clocks.stop()
-    dev_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
+    dev_ms = max_over_ranks(sum(step_ms), device="cuda")
     ms_per_step = dev_ms / args.steps
     value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
 

@@ -73,8 +73,12 @@ struct EriShape {
   static constexpr int SM_G = 3 * NR * GSZ;
   static constexpr int SM_BUFA = MI * NTUP;
   static constexpr int SM_BUFB = MI * MJ * NFK * NFL;
+  // small classes with few lanes run each (axis, root) recurrence in registers and write only
+  // the final I values to shared memory; the others keep the 2D table in shared memory (with
+  // 4+ lanes the unrolled form spills under the 128-register cap and measured slower)
+  static constexpr bool REG_RECUR = S <= 2 && NIJ * NKL <= 16 && GSZ <= 36;
   static constexpr int NTASK_CONC = S < 3 * NR ? S : 3 * NR;  // tasks running at once
-  static constexpr int SM_SCR = NTASK_CONC * NIJ * NKL;          // per-task 2D tables
+  static constexpr int SM_SCR = REG_RECUR ? 0 : NTASK_CONC * NIJ * NKL;  // per-task 2D tables
   // classes whose transform buffers do not fit on chip keep them in a per-block global scratch
   static constexpr bool GLOBAL_BUF = S > 1 && (SM_BUFA + SM_BUFB) * 8 * (S >= 128 ? 1 : 128 / S) > 200 * 1024;
   static constexpr int GBUF_PER_BLOCK = GLOBAL_BUF ? SM_BUFA + SM_BUFB : 0;
@@ -86,9 +90,10 @@ struct EriShape {
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : 65536 / (BLOCK * 128);
   static constexpr int Q = BLOCK / S;
-  // one-lane classes of low order stage their root-table block in shared memory: the lanes'
-  // scattered coefficient loads then cost shared-memory wavefronts instead of L1 sectors
-  static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
+  // classes of low order stage their root-table block in shared memory (before the groups'
+  // regions): the lanes' scattered coefficient loads then cost shared-memory wavefronts
+  // instead of L1 sectors
+  static constexpr bool STAGE_TABLE = NR <= 3;
   static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
   static constexpr int SMEM_BYTES = Q * SM_GROUP * 8 + TABLE_DOUBLES * 8;
 };
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
   extern __shared__ __align__(16) double smem[];
   const int group = threadIdx.x / S;
   const int lane = threadIdx.x % S;
-  double* sg = smem + group * SH::SM_GROUP;
+  double* sg = smem + SH::TABLE_DOUBLES + group * SH::SM_GROUP;
   double* s_roots = sg;                 // t2[NR], w[NR]
   double* s_g = sg + SH::SM_ROOTS;      // [axis][root][GSZ]
   double* s_scr = s_g + SH::SM_G;       // per-lane 2D tables (lanes < 3*NR)
@@ -384,7 +389,11 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
           groots = r_roots;
           gg = r_g;
         } else {
-          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+          if constexpr (SH::STAGE_TABLE) {
+            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
+          } else {
+            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+          }
           group_sync<S>(group);
           groots = s_roots;
           gg = s_g;
@@ -422,8 +431,13 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
             const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
             const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
             const double g00 = axis == 2 ? groots[NR + r] * fac : 1.0;
-            vrr_hrr_smem<LI, LJ, LK, LL>(gg + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), g00,
-                                         pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01, b00, ab, cd);
+            if constexpr (SH::REG_RECUR) {
+              vrr_hrr<LI, LJ, LK, LL>(gg + task * GSZ, g00, pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01,
+                                      b00, ab, cd);
+            } else {
+              vrr_hrr_smem<LI, LJ, LK, LL>(gg + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), g00,
+                                           pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01, b00, ab, cd);
+            }
           }
           group_sync<S>(group);
         }

@@ -101,3 +101,25 @@ __device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable
     else w[f - N] = acc;
   }
 }
+
+// As rys_fn for order N, with the coefficient block staged in shared memory at `tab`.
+template <int N>
+__device__ __forceinline__ double rys_fn_staged(const double* tab, const RysTable& c_rys, int f, double x) {
+  constexpr int xmax = cintx_rys_xmax(N);
+  if (!(x < (double)xmax)) {  // also routes NaN away from the table index
+    const double* a = c_rys.asym[N];
+    return f < N ? __ldg(a + f) / x : __ldg(a + f) * rsqrt(x);
+  }
+  const int i = (int)x;
+  const double z = 2.0 * (x - (double)i) - 1.0;
+  const double2* c2 = reinterpret_cast<const double2*>(tab + ((size_t)i * 2 * N + f) * RYS_NC);
+  const double2 hi = c2[RYS_NC / 2 - 1];
+  double acc = fma(hi.y, z, hi.x);
+#pragma unroll
+  for (int k = RYS_NC / 2 - 2; k >= 0; --k) {
+    const double2 v = c2[k];
+    acc = fma(acc, z, v.y);
+    acc = fma(acc, z, v.x);
+  }
+  return acc;
+}

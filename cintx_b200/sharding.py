@@ -1,0 +1,39 @@
+"""Multi-GPU sharding of a screened sweep.
+
+Shell quartets are independent and write disjoint output blocks, so a sweep shards with no
+data exchange: every rank builds the same plan (deterministic from the same inputs), takes the
+chunks `assign_chunks` gives it, and the only collectives are a barrier around the timed region
+and a max-reduction of the step time (`max_over_ranks`).
+"""
+from __future__ import annotations
+
+
+def assign_chunks(costs, nranks: int):
+    """Longest-first greedy assignment of chunks (by cost estimate) to ranks.
+
+    Returns owner[c] for every chunk; identical on every rank for identical costs.
+    """
+    order = sorted(range(len(costs)), key=lambda c: (-costs[c], c))
+    load = [0.0] * nranks
+    owner = [0] * len(costs)
+    for c in order:
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        owner[c] = r
+        load[r] += costs[c]
+    return owner
+
+
+def chunks_of(owner, rank: int):
+    return [c for c, r in enumerate(owner) if r == rank]
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """Max of a per-rank scalar over the default process group (the value itself when the
+    group is not initialised)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
