@@ -17,6 +17,8 @@
 // angular momentum, libcint's ibase/kbase choice, g2e.c:98-116).  Output strides let a launch
 // write any requested index order of the block.
 #pragma once
+#include <utility>
+
 #include "common.h"
 #include "c2s_coef.h"
 #include "rys_roots.cuh"
@@ -90,10 +92,11 @@ struct EriShape {
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : 65536 / (BLOCK * 128);
   static constexpr int Q = BLOCK / S;
-  // classes of low order stage their root-table block in shared memory (before the groups'
-  // regions): the lanes' scattered coefficient loads then cost shared-memory wavefronts
-  // instead of L1 sectors
-  static constexpr bool STAGE_TABLE = NR <= 3;
+  // one-lane classes of low order stage their root-table block in shared memory: the lanes'
+  // scattered coefficient loads then cost shared-memory wavefronts instead of L1 sectors
+  // (multi-lane groups evaluate each root once per group; a per-block copy there costs more
+  // occupancy than it saves, measured)
+  static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
   static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
   static constexpr int SMEM_BYTES = Q * SM_GROUP * 8 + TABLE_DOUBLES * 8;
 };
@@ -256,6 +259,28 @@ __device__ __forceinline__ void decode_tuples(LaneTuples<SH>& lt, int lane) {
   }
 }
 
+// Calls f(std::integral_constant<int, I>) for I = 0..N-1 in order (compile-time unrolling).
+template <class F, int... I>
+__device__ __forceinline__ void static_loop(std::integer_sequence<int, I...>, F&& f) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+
+// Compile-time offsets of every (fj, fk, fl) tuple into the I arrays, for the one-lane path
+// (runtime offsets would force its register arrays into local memory).
+template <class SH, int LJ, int LK, int LL>
+struct TupleOffsets {
+  int ox[SH::NTUP], oy[SH::NTUP], oz[SH::NTUP];
+  constexpr TupleOffsets() : ox(), oy(), oz() {
+    constexpr int SJ = SH::NI, SK = SH::NI * SH::NJ, SL = SH::NI * SH::NJ * SH::NK;
+    for (int t = 0; t < SH::NTUP; ++t) {
+      const int fj = t % SH::NFJ, fk = (t / SH::NFJ) % SH::NFK, fl = t / (SH::NFJ * SH::NFK);
+      ox[t] = cart_x(LJ, fj) * SJ + cart_x(LK, fk) * SK + cart_x(LL, fl) * SL;
+      oy[t] = cart_y(LJ, fj) * SJ + cart_y(LK, fk) * SK + cart_y(LL, fl) * SL;
+      oz[t] = cart_z(LJ, fj) * SJ + cart_z(LK, fk) * SK + cart_z(LL, fl) * SL;
+    }
+  }
+};
+
 // Primitive loop of the one-lane classes.  Quartets of a warp share their (ij) pair (row-major
 // tiles), so the inner loop's primitive-pair loads are warp-wide broadcasts; the lane's (kl)
 // primitive pair is loaded once per outer iteration.  `tab` is the shared-memory copy of the
@@ -307,14 +332,15 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
           vrr_hrr<LI, LJ, LK, LL>(gg + 1 * GSZ, 1.0, pay - ca * pqy, qcy + cb * pqy, b10, b01, b00, pij.aby, pkl.aby);
           vrr_hrr<LI, LJ, LK, LL>(gg + 2 * GSZ, w[r] * fac, paz - ca * pqz, qcz + cb * pqz, b10, b01, b00, pij.abz,
                                   pkl.abz);
-#pragma unroll
-          for (int k = 0; k < TPT; ++k) {
-#pragma unroll
-            for (int fi = 0; fi < NFI; ++fi) {
-              acc[k][fi] = fma(gg[cart_x(LI, fi) + lt.ox[k]] * gg[GSZ + cart_y(LI, fi) + lt.oy[k]],
-                               gg[2 * GSZ + cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
-            }
-          }
+          // every index below is a constant expression, so gg and acc stay in registers
+          static_loop(std::make_integer_sequence<int, TPT * NFI>{}, [&](auto c) {
+            constexpr int k = decltype(c)::value / NFI, fi = decltype(c)::value % NFI;
+            constexpr TupleOffsets<SH, LJ, LK, LL> TO{};
+            constexpr int ix = cart_x(LI, fi) + TO.ox[k];
+            constexpr int iy = GSZ + cart_y(LI, fi) + TO.oy[k];
+            constexpr int iz = 2 * GSZ + cart_z(LI, fi) + TO.oz[k];
+            acc[k][fi] = fma(gg[ix] * gg[iy], gg[iz], acc[k][fi]);
+          });
         }
       }
     }

@@ -86,8 +86,7 @@ __device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable
   const int i = (int)x;
   const double z = 2.0 * (x - (double)i) - 1.0;
   const double* c = tab + (size_t)i * 2 * N * RYS_NC;
-#pragma unroll
-  for (int f = F0; f < F1; ++f) {
+  auto horner = [&](int f) {
     const double2* c2 = reinterpret_cast<const double2*>(c + f * RYS_NC);
     const double2 hi = c2[RYS_NC / 2 - 1];
     double acc = fma(hi.y, z, hi.x);
@@ -97,8 +96,15 @@ __device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable
       acc = fma(acc, z, v.y);
       acc = fma(acc, z, v.x);
     }
-    if (f < N) t2[f] = acc;
-    else w[f - N] = acc;
+    return acc;
+  };
+  // one root (its t^2 and weight polynomials) in flight at a time: the compiler barrier keeps
+  // the other roots' coefficient loads from being hoisted into registers ahead of use
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    if (F0 <= r) t2[r] = horner(r);
+    if (N + r < F1) w[r] = horner(N + r);
+    if (r + 1 < N) asm volatile("" ::: "memory");
   }
 }
 
