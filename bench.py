@@ -47,6 +47,10 @@ WORKLOADS = {
     "water3": (M.water_like, "3-atom water-like molecule (O + 2 H), all quartets above 1e-12"),
 }
 SCHWARZ = 1e-12
+# tuned form: quartets whose estimated FP32 error is below this use FP32 recurrences; off by default
+# (5e-11 selects 0.5% of the mol40 quartets and measures 4.6% slower: the FP64 pipe is not the bound)
+FP32_BUDGET = 0.0
+PRIM_BUDGET = 5e-11  # tuned form: bound on the skipped primitive terms of one block
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cint_cpu_bench")
 
@@ -61,6 +65,11 @@ def parse():
     ap.add_argument("--chunk-doubles", type=int, default=1 << 28)
     ap.add_argument("--branches", type=int, default=4)
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--form", default="tuned", choices=["tuned", "plain"])
+    ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--error-chunks", type=int, default=4)
+    ap.add_argument("--fp32-budget", type=float, default=FP32_BUDGET)
+    ap.add_argument("--prim-budget", type=float, default=PRIM_BUDGET)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -251,35 +260,13 @@ def fp64_peak(cx, torch):
     return best
 
 
-def our_arm(args):
-    import torch
+def timed_sweep(cx, torch, plan, mine, args, stream, local, world):
+    """Warm-up, then exactly args.steps timed passes of `plan` over the rank's chunks (one CUDA
+    graph per pass unless --no-graph), L2 flushed between passes outside the events."""
     import torch.distributed as dist
-
-    import cintx_b200 as cx
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    fn, desc = WORKLOADS[args.workload]
-    mol = fn()
-    opt = cx.Optimizer(mol.atm, mol.bas, mol.env)
-    plan = cx.Plan.screened(opt, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
     st = plan.stats
-    nchunks = st.nchunks
-    seg_info = [plan.segments(c) for c in range(nchunks)]
-    chunk_flops = [float(s[2].sum()) for s in seg_info]
-    owner = assign_chunks(chunk_flops, world)
-    mine = chunks_of(owner, rank)
-    my_ints = sum(plan.chunk_size(c) for c in mine)
-    stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
-    torch.cuda.set_stream(stream)
     ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-
     use_graph = not args.no_graph
     if use_graph:
         try:
@@ -319,14 +306,15 @@ def our_arm(args):
     t_wall = time.perf_counter() - t_wall
     launches = cx.launch_count() - launches0
     clk = clocks.stop()
-    dev_ms = max_over_ranks(sum(step_ms), device="cuda")
-    ms_per_step = dev_ms / args.steps
-    value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
+    ms = max_over_ranks(sum(step_ms), device="cuda") / args.steps
+    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": ring}
 
-    # per-class profile of one step (segments timed individually)
+
+def class_profile(torch, plan, mine, ring, stream):
+    """One pass with every class segment timed on its own."""
     per_class = {}
     for c in mine:
-        cls, nq, fl = seg_info[c]
+        cls, nq, fl = plan.segments(c)
         for s in range(len(nq)):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -340,6 +328,81 @@ def our_arm(args):
             d["quartets"] += int(nq[s])
             d["launches"] += 1
             d["ints"] += int(nq[s]) * int(np.prod([2 * l + 1 for l in cls[s]]))
+    return per_class
+
+
+def tuned_error(cx, torch, opt, plan, ring, stream, max_chunks):
+    """Max and RMS absolute difference between the mixed plan and an FP64 evaluation of the same
+    quartets (explicit FP64 plan over each checked chunk's quartet list)."""
+    st = plan.stats
+    chunks = list(range(st.nchunks))
+    if len(chunks) > max_chunks:
+        chunks = sorted(set(np.linspace(0, st.nchunks - 1, max_chunks).astype(int).tolist()))
+    mx, ss, n = 0.0, 0.0, 0
+    for c in chunks:
+        plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
+        stream.synchronize()
+        got = ring[:plan.chunk_size(c)]
+        ref_plan = cx.Plan.shells(opt, cx.INT2E, plan.chunk_quartets(c), sph=True)
+        ref = torch.empty(ref_plan.stats.nintegrals, dtype=torch.float64, device="cuda")
+        ref_plan.execute(ref.data_ptr(), stream=stream.cuda_stream)
+        stream.synchronize()
+        d = (got - ref).abs()
+        mx = max(mx, float(d.max()))
+        ss += float((d * d).sum())
+        n += d.numel()
+        ref_plan.close()
+    return {"max_abs": mx, "rms_abs": (ss / max(n, 1)) ** 0.5, "integrals_checked": n,
+            "chunks_checked": len(chunks), "reference": "the same quartets evaluated by the FP64 kernels"}
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import cintx_b200 as cx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    fn, desc = WORKLOADS[args.workload]
+    mol = fn()
+    opt = cx.Optimizer(mol.atm, mol.bas, mol.env)
+    tuned = args.form == "tuned"
+
+    def make_plan(o, tuned_form):
+        if tuned_form:
+            return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=args.fp32_budget, prim_budget=args.prim_budget,
+                                          max_chunk_doubles=args.chunk_doubles)
+        return cx.Plan.screened(o, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
+
+    plan = make_plan(opt, tuned)
+    st = plan.stats
+    nchunks = st.nchunks
+    chunk_flops = [float(plan.segments(c)[2].sum()) for c in range(nchunks)]
+    mine = chunks_of(assign_chunks(chunk_flops, world), rank)
+    my_ints = sum(plan.chunk_size(c) for c in mine)
+    stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
+    torch.cuda.set_stream(stream)
+
+    main_run = timed_sweep(cx, torch, plan, mine, args, stream, local, world)
+    ms_per_step = main_run["ms"]
+    value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
+    plain = None
+    if tuned:
+        pplan = make_plan(opt, False)
+        pst = pplan.stats
+        pmine = chunks_of(assign_chunks([float(pplan.segments(c)[2].sum()) for c in range(pst.nchunks)], world), rank)
+        prun = timed_sweep(cx, torch, pplan, pmine, args, stream, local, world)
+        plain = {"value": pst.nintegrals / (prun["ms"] * 1e-3) / 1e9, "ms_per_step": prun["ms"]}
+        pplan.close()
+        del prun
+
+    per_class = class_profile(torch, plan, mine, main_run["ring"], stream)
     peak64 = fp64_peak(cx, torch)
     top = max(per_class.items(), key=lambda kv: kv[1]["ms"]) if per_class else (None, None)
     roof = None
@@ -352,6 +415,9 @@ def our_arm(args):
                 "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "share_of_step": d["ms"] / prof_total, "traffic": None,
                 "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
+    err = None
+    if tuned and rank == 0 and not args.no_error:
+        err = tuned_error(cx, torch, opt, plan, main_run["ring"], stream, args.error_chunks)
     if rank != 0:
         if world > 1:
             dist.barrier()
@@ -363,28 +429,38 @@ def our_arm(args):
         hbm = json.load(open(PEAKS_FILE))["hbm_gbs"]
     except Exception:
         pass
-    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (plain FP64 form)", "value": value, "unit": "Gint/s",
+    form = ("tuned: primitive Schwarz screening (budget %g per integral), FP32 recurrences where the estimated "
+            "FP32 error is below %g, "
+            "graph-batched" % (args.prim_budget, args.fp32_budget)) if tuned else "plain FP64"
+    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (%s form)" % ("tuned" if tuned else "plain FP64"),
+            "value": value, "unit": "Gint/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded molecule; no dataset)",
-            "config": {"workload": args.workload, "description": desc, "form": "plain_fp64",
-                       "nquartets": st.nquartets, "nintegrals": st.nintegrals, "nchunks": nchunks,
+            "config": {"workload": args.workload, "description": desc, "form": form,
+                       "nquartets": st.nquartets, "nquartets_fp32": st.nquartets_fp32,
+                       "nintegrals": st.nintegrals, "nchunks": nchunks,
                        "chunk_doubles": args.chunk_doubles, "schwarz_cutoff": SCHWARZ,
                        "nprim_quartets": st.nprim_quartets, "model_flops_per_step": st.flops,
                        "l2": "flushed between steps (512 MiB write outside the step events); each step also "
                              "streams %.1f GB of output through HBM" % (st.nintegrals * 8 / 1e9)},
             "quartets_per_s": st.nquartets / (ms_per_step * 1e-3),
-            "gpu_launches": launches,
-            "clocks": clk, "wall_s_timed_region": t_wall,
+            "gpu_launches": main_run["launches"],
+            "clocks": main_run["clocks"], "wall_s_timed_region": main_run["wall"],
             "roofline": roof,
             "output_write_gbs": st.nintegrals * 8 / (ms_per_step * 1e-3) / 1e9,
             "hbm_gbs_measured_peak": hbm,
             "execution": "one CUDA graph per step (%d kernel classes on %d branches)" % (len(per_class), args.branches)
-                         if use_graph else "direct launches",
+                         if main_run["graph"] else "direct launches",
             "per_class": {k: {"ms": round(v["ms"], 4), "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3),
                               "gint_s": round(v["ints"] / (v["ms"] * 1e-3) / 1e9, 2), "quartets": v["quartets"]}
                           for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:16]},
             "profiled_step_ms": sum(v["ms"] for v in per_class.values())}
+    if plain is not None:
+        line["plain_fp64"] = plain
+        line["tuned_over_plain"] = value / plain["value"]
+    if err is not None:
+        line["error_vs_fp64"] = err
 
     # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1)
     if not args.no_e2e:
@@ -395,7 +471,7 @@ def our_arm(args):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             o2 = cx.Optimizer(mol.atm, mol.bas, mol.env)
-            p2 = cx.Plan.screened(o2, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
+            p2 = make_plan(o2, tuned)
             for c in mine:
                 p2.execute_host(host, chunk=c)
             t1 = time.perf_counter()

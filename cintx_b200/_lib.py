@@ -27,7 +27,7 @@ class CintxError(RuntimeError):
 class PlanStats(ctypes.Structure):
     _fields_ = [("nquartets", _i64), ("nintegrals", _i64), ("nchunks", _i64),
                 ("max_chunk_doubles", _i64), ("nprim_quartets", _i64), ("device_bytes", _i64),
-                ("flops", _d)]
+                ("nquartets_fp32", _i64), ("flops", _d)]
 
 
 def _load() -> ctypes.CDLL:
@@ -58,6 +58,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_shells.restype = _i
     L.cintx_plan_int2e_screened.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64]
     L.cintx_plan_int2e_screened.restype = _i
+    L.cintx_plan_int2e_screened_mixed.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64, _d, _d]
+    L.cintx_plan_int2e_screened_mixed.restype = _i
     L.cintx_plan_stats.argtypes = [_vp, ctypes.POINTER(PlanStats)]
     L.cintx_plan_stats.restype = _i
     L.cintx_plan_chunk_size.argtypes = [_vp, _i64]
@@ -241,6 +243,18 @@ class Plan:
         h = _vp()
         _check(lib.cintx_plan_int2e_screened(ctypes.byref(h), opt.handle, float(cutoff), int(sph),
                                              int(max_chunk_doubles)))
+        return cls(h, opt)
+
+    @classmethod
+    def screened_mixed(cls, opt: Optimizer, cutoff: float = 1e-12, fp32_budget: float = 0.0,
+                       prim_budget: float = 5e-11, max_chunk_doubles: int = 1 << 28):
+        """Tuned sweep: primitive Schwarz screening within prim_budget per integral and, when
+        fp32_budget > 0, FP32 recurrences for quartets whose estimated FP32 error (primitive-
+        absolute Schwarz bound times the recurrences' cancellation factor) is below fp32_budget."""
+        h = _vp()
+        _check(lib.cintx_plan_int2e_screened_mixed(ctypes.byref(h), opt.handle, float(cutoff), 1,
+                                                   int(max_chunk_doubles), float(fp32_budget),
+                                                   float(prim_budget)))
         return cls(h, opt)
 
     @property

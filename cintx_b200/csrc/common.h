@@ -19,13 +19,15 @@ __host__ __device__ constexpr int cintx_rys_xmax(int n) {
 // One primitive pair (a, b) of an oriented shell pair (i, j), after exponent screening.
 // kab folds exp(-a_i a_j/a_ij |A-B|^2), both contraction coefficients (single contraction)
 // and the pair's share of libcint's common factor sqrt(2 pi^2.5) * fac_sp(li) * fac_sp(lj).
+// When q is set, a shell pair's primitive pairs are sorted by decreasing q, so a primitive
+// quartet loop can stop at the first pair whose bound q_ab * q_cd falls below its threshold.
 struct __align__(64) PrimPair {
   double aij;         // a_i + a_j
   double px, py, pz;  // product centre P = (a_i A + a_j B) / a_ij
   double kab;         // prefactor described above
   double cce;         // libcint screening exponent of this pair (CINTset_pairdata)
   double half_inv;    // 0.5 / a_ij
-  double pad;
+  double q;           // primitive Schwarz factor |c_i c_j| sqrt(max|(ab|ab)|) (0: not computed)
 };
 
 // An oriented shell pair (i, j).  Its primitive pairs are prims[prim_off, prim_off+nprim).
@@ -56,6 +58,7 @@ struct __align__(16) GenRange {
   long long rec_off;
   long long out_off;
   long long nout;
+  const int* colstart;  // per row: first column of the range's tile (nullptr: 0)
 };
 
 // Output placement of one launch group: the element (a, b, c, d) of the canonical block

@@ -6,7 +6,8 @@ namespace cintx {
 
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
-                         double expcutoff, const RysTable& rys, cudaStream_t stream) {
+                         double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32,
+                         double prim_eps) {
   LaunchArgs a;
   a.recs = recs;
   a.nrec = nrec;
@@ -18,6 +19,8 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
   a.rys = rys;
   a.stream = stream;
   a.max_blocks = 0;
+  a.fp32 = fp32;
+  a.prim_eps = prim_eps;
   return dispatch_eri(li, lj, lk, ll, sph, a);
 }
 

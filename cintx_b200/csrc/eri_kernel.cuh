@@ -17,6 +17,7 @@
 // angular momentum, libcint's ibase/kbase choice, g2e.c:98-116).  Output strides let a launch
 // write any requested index order of the block.
 #pragma once
+#include <type_traits>
 #include <utility>
 
 #include "common.h"
@@ -54,7 +55,7 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll) {
   return s;
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -84,9 +85,14 @@ struct EriShape {
   // classes whose transform buffers do not fit on chip keep them in a per-block global scratch
   static constexpr bool GLOBAL_BUF = S > 1 && (SM_BUFA + SM_BUFB) * 8 * (S >= 128 ? 1 : 128 / S) > 200 * 1024;
   static constexpr int GBUF_PER_BLOCK = GLOBAL_BUF ? SM_BUFA + SM_BUFB : 0;
-  static constexpr int SM_GROUP_RAW =
-      S == 1 ? 0 : cmax(SM_ROOTS + SM_G + SM_SCR, GLOBAL_BUF ? 0 : SM_BUFA + SM_BUFB);
-  static constexpr int SM_GROUP = (SM_GROUP_RAW + 1) & ~1;  // 16-byte multiple
+  // group region in bytes: roots (double) | I arrays and 2D tables (R) during the primitive
+  // loop; the transform buffers (double) alias it afterwards
+  static constexpr int B_ROOTS = SM_ROOTS * 8;
+  static constexpr int B_G = SM_G * (int)sizeof(R);
+  static constexpr int B_SCR = SM_SCR * (int)sizeof(R);
+  static constexpr int B_GROUP_RAW =
+      S == 1 ? 0 : cmax(B_ROOTS + B_G + B_SCR, GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8);
+  static constexpr int B_GROUP = (B_GROUP_RAW + 15) & ~15;
   static constexpr int BLOCK = S >= 128 ? S : 128;
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
   // multi-lane kernels (their stalls are latency bound and need warps)
@@ -98,7 +104,7 @@ struct EriShape {
   // occupancy than it saves, measured)
   static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
   static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
-  static constexpr int SMEM_BYTES = Q * SM_GROUP * 8 + TABLE_DOUBLES * 8;
+  static constexpr int SMEM_BYTES = Q * B_GROUP + TABLE_DOUBLES * 8;
 };
 
 // Group barrier: warp-level for S <= 32, a named barrier per group above.
@@ -117,31 +123,30 @@ __device__ __forceinline__ void group_sync(int group) {
 
 // 2D recurrence for one (axis, root) followed by the horizontal transfers; writes
 // I[i + NI*(j + NJ*(k + NK*l))] to dst (stride 1).
-template <int LI, int LJ, int LK, int LL>
-__device__ __forceinline__ void vrr_hrr(double* __restrict__ dst, double g00, double c00, double c0p,
-                                        double b10, double b01, double b00, double ab, double cd) {
+template <int LI, int LJ, int LK, int LL, class R = double>
+__device__ __forceinline__ void vrr_hrr(R* __restrict__ dst, R g00, R c00, R c0p, R b10, R b01, R b00, R ab, R cd) {
   constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
   constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
-  double G[NIJ][NKL];
+  R G[NIJ][NKL];
   G[0][0] = g00;
 #pragma unroll
   for (int n = 1; n < NIJ; ++n)
-    G[n][0] = c00 * G[n - 1][0] + (n > 1 ? (n - 1) * b10 * G[n - 2][0] : 0.0);
+    G[n][0] = c00 * G[n - 1][0] + (n > 1 ? (R)(n - 1) * b10 * G[n - 2][0] : (R)0);
 #pragma unroll
   for (int m = 1; m < NKL; ++m) {
 #pragma unroll
     for (int n = 0; n < NIJ; ++n) {
-      double v = c0p * G[n][m - 1];
-      if (m > 1) v += (m - 1) * b01 * G[n][m - 2];
-      if (n > 0) v += n * b00 * G[n - 1][m - 1];
+      R v = c0p * G[n][m - 1];
+      if (m > 1) v += (R)(m - 1) * b01 * G[n][m - 2];
+      if (n > 0) v += (R)n * b00 * G[n - 1][m - 1];
       G[n][m] = v;
     }
   }
-  double abp[LJ + 1], cdp[LL + 1];
-  abp[0] = 1.0;
+  R abp[LJ + 1], cdp[LL + 1];
+  abp[0] = (R)1;
 #pragma unroll
   for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
-  cdp[0] = 1.0;
+  cdp[0] = (R)1;
 #pragma unroll
   for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
 #pragma unroll
@@ -152,29 +157,28 @@ __device__ __forceinline__ void vrr_hrr(double* __restrict__ dst, double g00, do
       for (int j = 0; j <= LJ; ++j)
 #pragma unroll
         for (int i = 0; i <= LI; ++i) {
-          double v = 0.0;
+          R v = (R)0;
 #pragma unroll
           for (int a = 0; a <= j; ++a)
 #pragma unroll
             for (int b = 0; b <= l; ++b)
-              v += (double)(binom(j, a) * binom(l, b)) * abp[j - a] * cdp[l - b] * G[i + a][k + b];
+              v += (R)(binom(j, a) * binom(l, b)) * abp[j - a] * cdp[l - b] * G[i + a][k + b];
           dst[i + NI * (j + NJ * (k + NK * l))] = v;
         }
 }
 
 // Shared-memory version for the multi-lane path: the 2D table lives in gs[n*NKL + m]; the
 // horizontal transfers are unrolled over j and the (k, l) outputs, looped over i.
-template <int LI, int LJ, int LK, int LL>
-__device__ __forceinline__ void vrr_hrr_smem(double* __restrict__ dst, double* __restrict__ gs, double g00,
-                                             double c00, double c0p, double b10, double b01, double b00,
-                                             double ab, double cd) {
+template <int LI, int LJ, int LK, int LL, class R = double>
+__device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict__ gs, R g00, R c00, R c0p, R b10,
+                                             R b01, R b00, R ab, R cd) {
   constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
   constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
   {
-    double gm2 = 0.0, gm1 = g00;
+    R gm2 = (R)0, gm1 = g00;
     gs[0] = g00;
     for (int n = 1; n < NIJ; ++n) {
-      const double g = c00 * gm1 + (n - 1) * b10 * gm2;
+      const R g = c00 * gm1 + (R)(n - 1) * b10 * gm2;
       gs[n * NKL] = g;
       gm2 = gm1;
       gm1 = g;
@@ -182,37 +186,37 @@ __device__ __forceinline__ void vrr_hrr_smem(double* __restrict__ dst, double* _
   }
   for (int m = 1; m < NKL; ++m) {
     for (int n = 0; n < NIJ; ++n) {
-      double v = c0p * gs[n * NKL + m - 1];
-      if (m > 1) v += (m - 1) * b01 * gs[n * NKL + m - 2];
-      if (n > 0) v += n * b00 * gs[(n - 1) * NKL + m - 1];
+      R v = c0p * gs[n * NKL + m - 1];
+      if (m > 1) v += (R)(m - 1) * b01 * gs[n * NKL + m - 2];
+      if (n > 0) v += (R)n * b00 * gs[(n - 1) * NKL + m - 1];
       gs[n * NKL + m] = v;
     }
   }
-  double abp[LJ + 1], cdp[LL + 1];
-  abp[0] = 1.0;
+  R abp[LJ + 1], cdp[LL + 1];
+  abp[0] = (R)1;
 #pragma unroll
   for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
-  cdp[0] = 1.0;
+  cdp[0] = (R)1;
 #pragma unroll
   for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
   for (int i = 0; i <= LI; ++i) {
 #pragma unroll
     for (int j = 0; j <= LJ; ++j) {
-      double T[NKL];
+      R T[NKL];
 #pragma unroll
       for (int m = 0; m < NKL; ++m) {
-        double v = 0.0;
+        R v = (R)0;
 #pragma unroll
-        for (int a = 0; a <= j; ++a) v += (double)binom(j, a) * abp[j - a] * gs[(i + a) * NKL + m];
+        for (int a = 0; a <= j; ++a) v += (R)binom(j, a) * abp[j - a] * gs[(i + a) * NKL + m];
         T[m] = v;
       }
 #pragma unroll
       for (int l = 0; l <= LL; ++l)
 #pragma unroll
         for (int k = 0; k <= LK; ++k) {
-          double v = 0.0;
+          R v = (R)0;
 #pragma unroll
-          for (int b = 0; b <= l; ++b) v += (double)binom(l, b) * cdp[l - b] * T[k + b];
+          for (int b = 0; b <= l; ++b) v += (R)binom(l, b) * cdp[l - b] * T[k + b];
           dst[i + NI * (j + NJ * (k + NK * l))] = v;
         }
     }
@@ -285,18 +289,22 @@ struct TupleOffsets {
 // tiles), so the inner loop's primitive-pair loads are warp-wide broadcasts; the lane's (kl)
 // primitive pair is loaded once per outer iteration.  `tab` is the shared-memory copy of the
 // order-NR root table when SH::STAGE_TABLE (otherwise the global table is read).
-template <int LI, int LJ, int LK, int LL, class SH>
+template <int LI, int LJ, int LK, int LL, class SH, class R>
 __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const ShellPair& pkl,
                                                    const PrimPair* __restrict__ prims, const RysTable& rys,
-                                                   const double* tab, double expcutoff, const LaneTuples<SH>& lt,
-                                                   double (&acc)[SH::TPT][SH::NFI]) {
+                                                   const double* tab, double expcutoff, double prim_eps,
+                                                   const LaneTuples<SH>& lt, double (&acc)[SH::TPT][SH::NFI]) {
   constexpr int NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool SSSS = LI + LJ + LK + LL == 0;
   for (int b = 0; b < pkl.nprim; ++b) {
     const PrimPair pk = prims[pkl.prim_off + b];
     const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+    // primitive Schwarz screening: (ij) pairs are sorted by q, so stop at the first one whose
+    // bound q_ij * q_kl < prim_eps (prim_eps == 0 gives NaN or 0 here: never stops)
+    const double qthr = prim_eps / pk.q;
     for (int a = 0; a < pij.nprim; ++a) {
       const PrimPair pi = prims[pij.prim_off + a];
+      if (pi.q < qthr) break;
       if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
       const double aij = pi.aij, akl = pk.aij;
       const double aijkl = aij + akl;
@@ -320,18 +328,29 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
         acc[0][0] = fma(w[0], fac, acc[0][0]);  // (ss|ss) needs the weight only
       } else {
         const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
+        // reduced-precision classes sum the roots of one primitive quartet in R and add the sum
+        // to the FP64 accumulators (primitive accumulation stays FP64)
+        R part[std::is_same<R, double>::value ? 1 : TPT][std::is_same<R, double>::value ? 1 : NFI];
+        if constexpr (!std::is_same<R, double>::value) {
+#pragma unroll
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) part[k2][f2] = (R)0;
+        }
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          double gg[3 * GSZ];
+          R gg[3 * GSZ];
           const double rt_aa = t2[r] * inv_aijkl;
           const double b00 = 0.5 * rt_aa;
           const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
           const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
           const double ca = rt_aa * akl, cb = rt_aa * aij;
-          vrr_hrr<LI, LJ, LK, LL>(gg + 0 * GSZ, 1.0, pax - ca * pqx, qcx + cb * pqx, b10, b01, b00, pij.abx, pkl.abx);
-          vrr_hrr<LI, LJ, LK, LL>(gg + 1 * GSZ, 1.0, pay - ca * pqy, qcy + cb * pqy, b10, b01, b00, pij.aby, pkl.aby);
-          vrr_hrr<LI, LJ, LK, LL>(gg + 2 * GSZ, w[r] * fac, paz - ca * pqz, qcz + cb * pqz, b10, b01, b00, pij.abz,
-                                  pkl.abz);
+          vrr_hrr<LI, LJ, LK, LL, R>(gg + 0 * GSZ, (R)1, (R)(pax - ca * pqx), (R)(qcx + cb * pqx), (R)b10, (R)b01,
+                                     (R)b00, (R)pij.abx, (R)pkl.abx);
+          vrr_hrr<LI, LJ, LK, LL, R>(gg + 1 * GSZ, (R)1, (R)(pay - ca * pqy), (R)(qcy + cb * pqy), (R)b10, (R)b01,
+                                     (R)b00, (R)pij.aby, (R)pkl.aby);
+          vrr_hrr<LI, LJ, LK, LL, R>(gg + 2 * GSZ, (R)(w[r] * fac), (R)(paz - ca * pqz), (R)(qcz + cb * pqz),
+                                     (R)b10, (R)b01, (R)b00, (R)pij.abz, (R)pkl.abz);
           // every index below is a constant expression, so gg and acc stay in registers
           static_loop(std::make_integer_sequence<int, TPT * NFI>{}, [&](auto c) {
             constexpr int k = decltype(c)::value / NFI, fi = decltype(c)::value % NFI;
@@ -339,28 +358,38 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
             constexpr int ix = cart_x(LI, fi) + TO.ox[k];
             constexpr int iy = GSZ + cart_y(LI, fi) + TO.oy[k];
             constexpr int iz = 2 * GSZ + cart_z(LI, fi) + TO.oz[k];
-            acc[k][fi] = fma(gg[ix] * gg[iy], gg[iz], acc[k][fi]);
+            if constexpr (std::is_same<R, double>::value) acc[k][fi] = fma(gg[ix] * gg[iy], gg[iz], acc[k][fi]);
+            else part[k][fi] = fmaf(gg[ix] * gg[iy], gg[iz], part[k][fi]);
           });
+        }
+        if constexpr (!std::is_same<R, double>::value) {
+#pragma unroll
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) acc[k2][f2] += (double)part[k2][f2];
         }
       }
     }
   }
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape<LI, LJ, LK, LL, SPH>::MINB)
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R>::BLOCK, EriShape<LI, LJ, LK, LL, SPH, R>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
-                 double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH>;
+                 double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
+                 double prim_eps) {
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
+  constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];
   const int group = threadIdx.x / S;
   const int lane = threadIdx.x % S;
-  double* sg = smem + SH::TABLE_DOUBLES + group * SH::SM_GROUP;
-  double* s_roots = sg;                 // t2[NR], w[NR]
-  double* s_g = sg + SH::SM_ROOTS;      // [axis][root][GSZ]
-  double* s_scr = s_g + SH::SM_G;       // per-lane 2D tables (lanes < 3*NR)
+  char* sgb = reinterpret_cast<char*>(smem + SH::TABLE_DOUBLES) + group * SH::B_GROUP;
+  double* sg = reinterpret_cast<double*>(sgb);  // transform buffers after the primitive loop
+  double* s_roots = sg;                         // t2[NR], w[NR]
+  R* s_g = reinterpret_cast<R*>(sgb + SH::B_ROOTS);  // [axis][root][GSZ]
+  R* s_scr = s_g + SH::SM_G;                    // per-lane 2D tables (lanes < 3*NR)
 
   if constexpr (SH::STAGE_TABLE) {
     const double2* src = reinterpret_cast<const double2*>(rys.poly[NR]);
@@ -371,10 +400,6 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
 
   LaneTuples<SH> lt;
   decode_tuples<SH, LJ, LK, LL>(lt, lane);
-
-  // per-thread register storage used when S == 1
-  double r_roots[S == 1 ? 2 * NR : 1];
-  double r_g[S == 1 ? 3 * NR * GSZ : 1];
 
   for (int q = blockIdx.x * SH::Q + group; q < nrec; q += gridDim.x * SH::Q) {
     const QuartetRec rec = recs[q];
@@ -387,14 +412,16 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
       for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
 
     if constexpr (S == 1) {
-      prim_loop_one_lane<LI, LJ, LK, LL, SH>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff, lt,
-                                             acc);
+      prim_loop_one_lane<LI, LJ, LK, LL, SH, R>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff,
+                                                prim_eps, lt, acc);
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];
       const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+      const double qthr = prim_eps / pk.q;  // as in prim_loop_one_lane
       for (int a = 0; a < pij.nprim; ++a) {
         const PrimPair pi = prims[pij.prim_off + a];
+        if (pi.q < qthr) break;
         if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
         const double aij = pi.aij, akl = pk.aij;
         const double aijkl = aij + akl;
@@ -408,81 +435,71 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH>::BLOCK, EriShape
         const double fac = pi.kab * pk.kab * rs * inv_a1;
         const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
 
-        double* groots;
-        double* gg;
-        if constexpr (S == 1) {
-          rys_all<NR>(rys, x, r_roots, r_roots + NR);
-          groots = r_roots;
-          gg = r_g;
+        // roots: the group's lanes split the 2*NR table polynomials
+        if constexpr (SH::STAGE_TABLE) {
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
         } else {
-          if constexpr (SH::STAGE_TABLE) {
-            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+        }
+        group_sync<S>(group);
+        // (axis, root) recurrences, one per lane; coefficients in FP64, recurrences in R
+        for (int task = lane; task < 3 * NR; task += S) {
+          const int axis = task / NR, r = task % NR;
+          const double t2 = s_roots[r];
+          const double rt_aa = t2 * inv_aijkl;
+          const double b00 = 0.5 * rt_aa;
+          const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
+          const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
+          const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
+          const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
+          const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
+          const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
+          const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
+          const double g00 = axis == 2 ? s_roots[NR + r] * fac : 1.0;
+          if constexpr (SH::REG_RECUR) {
+            vrr_hrr<LI, LJ, LK, LL, R>(s_g + task * GSZ, (R)g00, (R)(pa - rt_aa * akl * pq),
+                                       (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab, (R)cd);
           } else {
-            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+            vrr_hrr_smem<LI, LJ, LK, LL, R>(s_g + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), (R)g00,
+                                            (R)(pa - rt_aa * akl * pq), (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01,
+                                            (R)b00, (R)ab, (R)cd);
           }
-          group_sync<S>(group);
-          groots = s_roots;
-          gg = s_g;
         }
-        // (axis, root) recurrences
-        if constexpr (S == 1) {
+        group_sync<S>(group);
+        // cartesian products, summed over roots (R), added to the FP64 accumulators
+        R part[FP64 ? 1 : TPT][FP64 ? 1 : NFI];
+        if constexpr (!FP64) {
 #pragma unroll
-          for (int task = 0; task < 3 * NR; ++task) {
-            const int axis = task / NR, r = task % NR;
-            const double t2 = groots[r];
-            const double rt_aa = t2 * inv_aijkl;
-            const double b00 = 0.5 * rt_aa;
-            const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
-            const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
-            const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
-            const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
-            const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
-            const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
-            const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
-            const double g00 = axis == 2 ? groots[NR + r] * fac : 1.0;
-            vrr_hrr<LI, LJ, LK, LL>(gg + task * GSZ, g00, pa - rt_aa * akl * pq, qc + rt_aa * aij * pq,
-                                    b10, b01, b00, ab, cd);
-          }
-        } else {
-          for (int task = lane; task < 3 * NR; task += S) {
-            const int axis = task / NR, r = task % NR;
-            const double t2 = groots[r];
-            const double rt_aa = t2 * inv_aijkl;
-            const double b00 = 0.5 * rt_aa;
-            const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
-            const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
-            const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
-            const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
-            const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
-            const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
-            const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
-            const double g00 = axis == 2 ? groots[NR + r] * fac : 1.0;
-            if constexpr (SH::REG_RECUR) {
-              vrr_hrr<LI, LJ, LK, LL>(gg + task * GSZ, g00, pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01,
-                                      b00, ab, cd);
-            } else {
-              vrr_hrr_smem<LI, LJ, LK, LL>(gg + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), g00,
-                                           pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10, b01, b00, ab, cd);
-            }
-          }
-          group_sync<S>(group);
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) part[k2][f2] = (R)0;
         }
-        // cartesian products, summed over roots
 #pragma unroll 1
         for (int r = 0; r < NR; ++r) {
-          const double* gx = gg + (0 * NR + r) * GSZ;
-          const double* gy = gg + (1 * NR + r) * GSZ;
-          const double* gz = gg + (2 * NR + r) * GSZ;
+          const R* gx = s_g + (0 * NR + r) * GSZ;
+          const R* gy = s_g + (1 * NR + r) * GSZ;
+          const R* gz = s_g + (2 * NR + r) * GSZ;
 #pragma unroll
           for (int k = 0; k < TPT; ++k) {
 #pragma unroll
             for (int fi = 0; fi < NFI; ++fi) {
-              acc[k][fi] = fma(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
-                               gz[cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
+              if constexpr (FP64) {
+                acc[k][fi] = fma(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
+                                 gz[cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
+              } else {
+                part[k][fi] = fmaf(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
+                                   gz[cart_z(LI, fi) + lt.oz[k]], part[k][fi]);
+              }
             }
           }
         }
-        if constexpr (S > 1) group_sync<S>(group);
+        if constexpr (!FP64) {
+#pragma unroll
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) acc[k2][f2] += (double)part[k2][f2];
+        }
+        group_sync<S>(group);
       }
     }
 

@@ -18,6 +18,8 @@ struct LaunchArgs {
   cudaStream_t stream;
   int max_blocks;  // grid cap (0: derived from the SM count)
   int query = 0;   // 1: launch nothing; return cudaErrorNotSupported if the class needs scratch
+  bool fp32 = false;  // FP32 recurrences and products (spherical output only)
+  double prim_eps = 0;  // primitive Schwarz threshold (0: no primitive screening beyond libcint's)
 };
 
 // Device scratch for classes whose transform buffers live in global memory: returns a buffer
@@ -32,11 +34,11 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 
 int device_sm_count();
 
-template <int LI, int LJ, int LK, int LL, bool SPH>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -56,7 +58,7 @@ cudaError_t launch_eri(const LaunchArgs& a) {
     if (!scratch) return cudaErrorMemoryAllocation;
   }
   kern<<<(unsigned)blocks, SH::BLOCK, SH::SMEM_BYTES, a.stream>>>(a.recs, a.nrec, a.pairs, a.prims, a.out,
-                                                                   a.st, a.expcutoff, a.rys, scratch);
+                                                                   a.st, a.expcutoff, a.rys, scratch, a.prim_eps);
   return cudaGetLastError();
 }
 
@@ -77,8 +79,10 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
     static_for<K.value + 1>([&](auto L) {
       constexpr int k = decltype(K)::value, l = decltype(L)::value;
       if constexpr (class_valid(LI, LJ, k, l)) {
-        if (lk == k && ll == l)
-          err = sph ? launch_eri<LI, LJ, k, l, true>(a) : launch_eri<LI, LJ, k, l, false>(a);
+        if (lk == k && ll == l) {
+          if (a.fp32) err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
+          else err = sph ? launch_eri<LI, LJ, k, l, true>(a) : launch_eri<LI, LJ, k, l, false>(a);
+        }
       }
     });
   });

@@ -128,6 +128,8 @@ void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
   out.b = b;
   out.la = A.l;
   out.prims.clear();
+  out.pa.clear();
+  out.pb.clear();
   out.min_cce = 1e300;
   const double sq_common = sqrt(2.0 * pow(kPi, 2.5));  // sqrt of pi^3 * 2/sqrt(pi)
   ShellPair& sp = out.sp;
@@ -147,6 +149,8 @@ void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
       pp.cce = 0;
       pp.half_inv = 0.5 / A.exps[p];
       out.prims.push_back(pp);
+      out.pa.push_back(p);
+      out.pb.push_back(0);
       out.min_cce = 0;
     }
   } else {
@@ -181,6 +185,8 @@ void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
         pp.cce = cce;
         pp.half_inv = 0.5 * inv;
         out.prims.push_back(pp);
+        out.pa.push_back(p);
+        out.pb.push_back(q);
         out.min_cce = std::min(out.min_cce, cce);
       }
     }
@@ -342,6 +348,8 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
   o->pair_lb.assign(ntot, 0);
   o->pair_nprim.assign(ntot, 0);
   o->pair_min_cce.assign(ntot, 0);
+  o->h_prim_a.clear();
+  o->h_prim_b.clear();
   PairHost ph;
   for (int u = 0; u < nv; ++u) {
     for (int v = 0; v <= u; ++v) {
@@ -352,6 +360,8 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
       ph.sp.prim_off = (int)prims.size();
       sps[id] = ph.sp;
       prims.insert(prims.end(), ph.prims.begin(), ph.prims.end());
+      o->h_prim_a.insert(o->h_prim_a.end(), ph.pa.begin(), ph.pa.end());
+      o->h_prim_b.insert(o->h_prim_b.end(), ph.pb.begin(), ph.pb.end());
       o->pair_a[id] = a;
       o->pair_b[id] = b;
       o->pair_la[id] = ph.la;
@@ -366,6 +376,8 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
     ph.sp.prim_off = (int)prims.size();
     sps[id] = ph.sp;
     prims.insert(prims.end(), ph.prims.begin(), ph.prims.end());
+    o->h_prim_a.insert(o->h_prim_a.end(), ph.pa.begin(), ph.pa.end());
+    o->h_prim_b.insert(o->h_prim_b.end(), ph.pb.begin(), ph.pb.end());
     o->pair_a[id] = v;
     o->pair_b[id] = -1;
     o->pair_la[id] = ph.la;
@@ -378,6 +390,8 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
     return CINTX_STATUS_MEMORY_LIMIT_EXCEEDED;
   }
   o->nprims_total = (int64_t)prims.size();
+  o->h_prims = prims;
+  o->prim_schwarz = false;
   free_opt_device(o);
   cudaGetDevice(&o->device);
   if (cudaMalloc(&o->d_pairs, sizeof(ShellPair) * sps.size()) != cudaSuccess ||

@@ -56,6 +56,7 @@ struct PairHost {
   double min_cce = 1e300;
   ShellPair sp{};
   std::vector<PrimPair> prims;
+  std::vector<int> pa, pb;  // primitive indices (within shells a and b) of each entry of prims
 };
 
 // Builds the screened primitive pairs of virtual shells (a, b), in that order (b < 0: unit).
@@ -75,6 +76,15 @@ struct Opt {
   ShellPair* d_pairs = nullptr;
   PrimPair* d_prims = nullptr;
   int64_t nprims_total = 0;
+  // host copies of the primitive pairs and their primitive indices, for the primitive
+  // Schwarz pass; pair_qp[pair] = sum of the pair's q (set once prim_schwarz is true)
+  std::vector<PrimPair> h_prims;
+  std::vector<int> h_prim_a, h_prim_b;
+  std::vector<double> pair_qp;
+  // pair_amp[pair] = max over its primitive pairs of (1 + |P - C| sqrt(2 a_ab))^(la + lb), C the
+  // farther of the two centres: how far the pair's recurrences can cancel below their terms
+  std::vector<double> pair_amp;
+  bool prim_schwarz = false;
   std::mutex mu;
   static constexpr uint64_t kMagic = 0x43494e5458423230ull;  // "CINTXB20"
 };
@@ -84,6 +94,9 @@ inline int pair_index(int u, int v) {  // unordered, u >= v
 }
 
 Opt* as_opt(CINTOpt* o);
+// Computes every stored primitive pair's Schwarz factor q (cartesian primitive diagonals on the
+// device), sorts each shell pair's primitive pairs by decreasing q and re-uploads them.
+int compute_prim_schwarz(Opt* o);
 int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env);
 
 // Per-device constants (Rys table) and per-thread scratch.
@@ -120,6 +133,7 @@ double flops_c2s(int li, int lj, int lk, int ll, bool sph);
 bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph);
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
-                         double expcutoff, const RysTable& rys, cudaStream_t stream);
+                         double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32 = false,
+                         double prim_eps = 0.0);
 
 }  // namespace cintx

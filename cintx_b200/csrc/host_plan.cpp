@@ -48,6 +48,8 @@ struct Segment {
   double flops = 0;        // algorithmic FP64 flops of the segment
   int range0 = 0;          // merged class segments (tile == -2): GenRange slice
   int nranges = 0;
+  bool fp32 = false;       // FP32 recurrences (mixed-precision plans)
+  double prim_eps = 0;     // primitive Schwarz threshold (tuned plans)
 };
 
 struct Chunk {
@@ -63,9 +65,13 @@ struct Tile {
   std::vector<int> rows, cols;          // pair ids
   std::vector<long long> row_prefix;    // size rows+1
   std::vector<long long> cum_np;        // prefix of primitive-pair counts over cols
+  std::vector<int> colstart;            // per row: first column (empty: 0 for every row)
+  bool fp32 = false;                    // evaluated with FP32 recurrences
   int* d_rows = nullptr;
   int* d_cols = nullptr;
   long long* d_prefix = nullptr;
+  int* d_colstart = nullptr;
+  int col0(size_t row) const { return colstart.empty() ? 0 : colstart[row]; }
 };
 
 }  // namespace
@@ -103,6 +109,8 @@ void free_plan_device(CintxPlan* p) {
     if (t.d_rows) cudaFree(t.d_rows);
     if (t.d_cols) cudaFree(t.d_cols);
     if (t.d_prefix) cudaFree(t.d_prefix);
+    if (t.d_colstart) cudaFree(t.d_colstart);
+    t.d_colstart = nullptr;
     t.d_rows = t.d_cols = nullptr;
     t.d_prefix = nullptr;
   }
@@ -357,7 +365,7 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
   for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
     const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
     cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
-                                 out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream);
+                                 out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps);
     if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -482,7 +490,7 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
       for (long long q = sg.t0; q < sg.t1; ++q, ++k) {
         if (k >= cap) return CINTX_STATUS_BUFFER_TOO_SMALL;
         const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
-        const int pa = t.rows[row], pb = t.cols[q - t.row_prefix[row]];
+        const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
         const Basis& B = o->basis;
         quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
         quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
@@ -534,7 +542,7 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
       const Tile& t = p->tiles[ti];
       const long long q = g - tp[ti];
       const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
-      const int pa = t.rows[row], pb = t.cols[q - t.row_prefix[row]];
+      const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
       quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
       quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
       quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
@@ -670,7 +678,169 @@ void cintx_plan_destroy(CintxPlan* p) {
   delete p;
 }
 
+}  // extern "C"
+
+namespace cintx {
+
+// Primitive Schwarz factors.  A primitive-per-shell copy of the basis (coefficient 1, no
+// exponent screening) gives every needed primitive diagonal block (ab|ab) in cartesian form on
+// the device; q_ab = |c_a c_b| sqrt(max|(ab|ab)|) then bounds every cartesian primitive integral
+// of a quartet, |c_a c_b c_c c_d (ab|cd)| <= q_ab q_cd (Cauchy-Schwarz for the Coulomb metric).
+int compute_prim_schwarz(Opt* o) {
+  std::lock_guard<std::mutex> lk(o->mu);
+  if (o->prim_schwarz) return CINTX_STATUS_SUCCESS;
+  const Basis& B = o->basis;
+  std::vector<int> pbase(B.nbas);
+  std::vector<int> bas;
+  std::vector<double> env = B.env;
+  env[PTR_EXPCUTOFF] = 1e6;  // keep every primitive pair: zero blocks must mean zero
+  int np = 0;
+  for (int sh = 0; sh < B.nbas; ++sh) {
+    const ShellInfo& S = B.sh[sh];
+    pbase[sh] = np;
+    for (int p = 0; p < S.nprim; ++p, ++np) {
+      const int pe = (int)env.size();
+      env.push_back(S.exps[p]);
+      const int pc = (int)env.size();
+      env.push_back(1.0);
+      const int row[8] = {S.atom, S.l, 1, 1, 0, pe, pc, 0};
+      bas.insert(bas.end(), row, row + 8);
+    }
+  }
+  // distinct primitive-shell pairs used by the stored primitive pairs (regular pairs only)
+  std::map<std::pair<int, int>, int> need;
+  std::vector<int> tuples;
+  std::vector<int> which(o->h_prims.size(), -1);
+  std::vector<ShellPair> sps(o->npairs + B.nvirt);
+  cudaMemcpy(sps.data(), o->d_pairs, sizeof(ShellPair) * sps.size(), cudaMemcpyDeviceToHost);
+  for (int id = 0; id < o->npairs; ++id) {
+    const int sa = B.vshell[o->pair_a[id]], sb = B.vshell[o->pair_b[id]];
+    for (int k = sps[id].prim_off; k < sps[id].prim_off + sps[id].nprim; ++k) {
+      const int u = pbase[sa] + o->h_prim_a[k], v = pbase[sb] + o->h_prim_b[k];
+      auto key = std::make_pair(u, v);
+      auto it = need.find(key);
+      if (it == need.end()) {
+        it = need.emplace(key, (int)(tuples.size() / 4)).first;
+        const int t[4] = {u, v, u, v};
+        tuples.insert(tuples.end(), t, t + 4);
+      }
+      which[k] = it->second;
+    }
+  }
+  const int64_t nt = (int64_t)tuples.size() / 4;
+  std::vector<double> qprim(nt, 0.0);
+  if (nt > 0) {
+    Opt po;
+    po.magic = Opt::kMagic;
+    int rc = build_opt(&po, B.atm.data(), B.natm, bas.data(), np, env.data());
+    if (rc) return rc;
+    CintxPlan* pp = nullptr;
+    std::vector<int64_t> offs(nt);
+    rc = cintx_plan_shells(&pp, reinterpret_cast<CINTOpt*>(&po), CINTX_INT2E, tuples.data(), nt, 0, offs.data());
+    if (!rc) {
+      std::vector<double> outv(std::max<int64_t>(pp->stats.nintegrals, 1));
+      rc = cintx_plan_execute_host(pp, 0, outv.data());
+      const int64_t tot = pp->stats.nintegrals;
+      cintx_plan_destroy(pp);
+      if (!rc) {
+        for (int64_t t = 0; t < nt; ++t) {
+          const int64_t e1 = t + 1 < nt ? offs[t + 1] : tot;
+          double m = 0;
+          for (int64_t e = offs[t]; e < e1; ++e) m = std::max(m, fabs(outv[e]));
+          qprim[t] = sqrt(m);
+        }
+      }
+    }
+    if (po.d_pairs) cudaFree(po.d_pairs);
+    if (po.d_prims) cudaFree(po.d_prims);
+    po.magic = 0;
+    if (rc) return rc;
+  }
+  // q per stored primitive pair, sorted by decreasing q within each shell pair
+  o->pair_qp.assign(o->npairs + B.nvirt, 0.0);
+  o->pair_amp.assign(o->npairs + B.nvirt, 1.0);
+  for (int id = 0; id < o->npairs; ++id) {
+    const int a = o->pair_a[id], b = o->pair_b[id];
+    const ShellInfo& SA = B.sh[B.vshell[a]];
+    const ShellInfo& SB = B.sh[B.vshell[b]];
+    const int ca = B.vctr[a], cb = B.vctr[b];
+    const int k0 = sps[id].prim_off, n = sps[id].nprim;
+    std::vector<int> ord(n);
+    std::vector<double> qv(n);
+    double sum = 0, amp = 1.0;
+    for (int i = 0; i < n; ++i) {
+      const int k = k0 + i;
+      const double cab = fabs(SA.coef[(size_t)ca * SA.nprim + o->h_prim_a[k]] * SB.coef[(size_t)cb * SB.nprim + o->h_prim_b[k]]);
+      qv[i] = cab * qprim[which[k]];
+      ord[i] = i;
+      sum += qv[i];
+      const PrimPair& pp = o->h_prims[k];
+      const double da = sqrt((pp.px - SA.r[0]) * (pp.px - SA.r[0]) + (pp.py - SA.r[1]) * (pp.py - SA.r[1]) +
+                             (pp.pz - SA.r[2]) * (pp.pz - SA.r[2]));
+      const double db = sqrt((pp.px - SB.r[0]) * (pp.px - SB.r[0]) + (pp.py - SB.r[1]) * (pp.py - SB.r[1]) +
+                             (pp.pz - SB.r[2]) * (pp.pz - SB.r[2]));
+      amp = std::max(amp, pow(1.0 + std::max(da, db) * sqrt(2.0 * pp.aij), SA.l + SB.l));
+    }
+    o->pair_amp[id] = amp;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return qv[x] > qv[y]; });
+    std::vector<PrimPair> pp(n);
+    std::vector<int> pa(n), pb(n);
+    for (int i = 0; i < n; ++i) {
+      pp[i] = o->h_prims[k0 + ord[i]];
+      pp[i].q = qv[ord[i]];
+      pa[i] = o->h_prim_a[k0 + ord[i]];
+      pb[i] = o->h_prim_b[k0 + ord[i]];
+    }
+    for (int i = 0; i < n; ++i) {
+      o->h_prims[k0 + i] = pp[i];
+      o->h_prim_a[k0 + i] = pa[i];
+      o->h_prim_b[k0 + i] = pb[i];
+    }
+    o->pair_qp[id] = sum;
+  }
+  if (!o->h_prims.empty() &&
+      cudaMemcpy(o->d_prims, o->h_prims.data(), sizeof(PrimPair) * o->h_prims.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "upload of sorted primitive pairs failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  o->prim_schwarz = true;
+  return CINTX_STATUS_SUCCESS;
+}
+
+}  // namespace cintx
+
+extern "C" {
+
+static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk,
+                          double fp32_budget, double prim_budget);
+
 int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk) {
+  return build_screened(plan, optp, cutoff, sph, max_chunk, 0.0, 0.0);
+}
+
+int cintx_plan_int2e_screened_mixed(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk,
+                                    double fp32_budget, double prim_budget) {
+  if (fp32_budget > 0 && !sph) {
+    set_error(CINTX_STATUS_UNSUPPORTED_REPRESENTATION, "FP32 quartets are compiled for spherical output only");
+    return CINTX_STATUS_UNSUPPORTED_REPRESENTATION;
+  }
+  return build_screened(plan, optp, cutoff, sph, max_chunk, fp32_budget, prim_budget);
+}
+
+// FP32 error model of one quartet: 64 * 2^-24 per unit of bound (a factor 5 above the largest
+// error/bound seen in the FP32 emulation of the recurrences)
+static constexpr double kFp32ErrScale = 64.0 / 16777216.0;
+
+// Largest row 1-norm of the cartesian -> spherical transform of angular momentum l: an error
+// bound on cartesian blocks grows by at most this factor per axis in the spherical block.
+static double c2s_amp(int l, bool sph) {
+  static const double amp[5] = {1.0, 1.0, 1.26156626101008, 2.985410660720923, 7.569397566060481};
+  return sph && l >= 2 ? amp[std::min(l, 4)] : 1.0;
+}
+
+static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk,
+                          double fp32_budget, double prim_budget) {
   clear_error();
   if (!plan) {
     set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
@@ -692,6 +862,10 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
     return CINTX_STATUS_UNSUPPORTED_API;
   }
   if (max_chunk <= 0) max_chunk = 1LL << 28;
+  if (fp32_budget > 0 || prim_budget > 0) {
+    int rc0 = compute_prim_schwarz(o);
+    if (rc0) return rc0;
+  }
   const int np = o->npairs;
   const int nb = B.nbas;
   // 1. Schwarz factors from the diagonal (ij|ij) blocks, cartesian-free (sph) evaluation
@@ -741,7 +915,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
   p->family = CINTX_INT2E;
   p->sph = sph != 0;
   const double ecut = expcutoff_2e(B.env.data());
-  long long nq_total = 0, nint_total = 0, nprimq = 0;
+  long long nq_total = 0, nint_total = 0, nprimq = 0, nq_fp32 = 0;
   double flops = 0;
   const int nt = (int)tlist.size();
   // tiles A >= B in type order (types are ordered by (la, lb, ...), so classes are valid)
@@ -760,7 +934,27 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       for (size_t c = 0; c < cols.size(); ++c) qcols[c] = Q[cols[c]];
       std::vector<long long> cum_np(cols.size() + 1, 0);
       for (size_t c = 0; c < cols.size(); ++c) cum_np[c + 1] = cum_np[c] + o->pair_nprim[cols[c]];
+      // FP32 recurrences only where they replace real work (total l >= 4) and where the estimated
+      // FP32 error of the quartet, kFp32ErrScale * (qp amp)_ab * (qp amp)_cd * c2s amplification,
+      // stays below fp32_budget.  qp is the primitive-absolute bound sum_ab q_ab; amp bounds the
+      // cancellation of the recurrences (checked against an FP32 emulation of the recurrences on
+      // random quartets of mixed-exponent molecules: the error stayed below 12 * 2^-24 * bound * amp).
+      const bool fp32_class = fp32_budget > 0 && t.li + t.lj + t.lk + t.ll >= 4;
+      const double fp32_thr =
+          fp32_budget / (kFp32ErrScale * c2s_amp(t.li, p->sph) * c2s_amp(t.lj, p->sph) * c2s_amp(t.lk, p->sph) *
+                         c2s_amp(t.ll, p->sph));
+      // suffix maxima of qp*amp over the Q-sorted columns: the FP32 tail of a row starts where
+      // (qp amp)_row * (largest qp amp still ahead) < fp32_thr
+      std::vector<double> qp_sufmax(cols.size() + 1, 0.0);
+      if (fp32_class)
+        for (size_t c = cols.size(); c-- > 0;)
+          qp_sufmax[c] = std::max(qp_sufmax[c + 1], o->pair_qp[cols[c]] * o->pair_amp[cols[c]]);
+      // each row's partner prefix [0, cnt) splits into FP64 columns [0, c64) and FP32 columns
+      // [c64, cnt)
+      Tile t32 = t;
+      t32.fp32 = true;
       t.row_prefix.push_back(0);
+      t32.row_prefix.push_back(0);
       for (size_t r = 0; r < rows.size(); ++r) {
         const double qa = Q[rows[r]];
         // count of cols with qa * Q >= cutoff (cols sorted decreasing)
@@ -768,19 +962,35 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
                         qcols.begin();
         if (A == Bt) cnt = std::min<long long>(cnt, (long long)r + 1);
         if (cnt <= 0) continue;
-        t.rows.push_back(rows[r]);
-        t.row_prefix.push_back(t.row_prefix.back() + cnt);
-        nprimq += (long long)o->pair_nprim[rows[r]] * cum_np[cnt];
+        long long c64 = cnt;
+        if (fp32_class) {
+          const double qpa = o->pair_qp[rows[r]] * o->pair_amp[rows[r]];
+          c64 = std::partition_point(qp_sufmax.begin(), qp_sufmax.begin() + cols.size(),
+                                     [&](double m) { return qpa * m >= fp32_thr; }) - qp_sufmax.begin();
+          c64 = std::min(c64, cnt);
+        }
+        if (c64 > 0) {
+          t.rows.push_back(rows[r]);
+          t.row_prefix.push_back(t.row_prefix.back() + c64);
+        }
+        if (cnt > c64) {
+          t32.rows.push_back(rows[r]);
+          t32.colstart.push_back((int)c64);
+          t32.row_prefix.push_back(t32.row_prefix.back() + (cnt - c64));
+        }
       }
-      if (t.rows.empty()) continue;
-      t.cols = cols;
-      t.cum_np = cum_np;
-      const long long nq = t.row_prefix.back();
       const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
                              nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
-      nq_total += nq;
-      nint_total += nq * nout;
-      p->tiles.push_back(t);
+      for (Tile* tp : {&t, &t32}) {
+        if (tp->rows.empty()) continue;
+        tp->cols = cols;
+        tp->cum_np = cum_np;
+        const long long nq = tp->row_prefix.back();
+        nq_total += nq;
+        nint_total += nq * nout;
+        if (tp->fp32) nq_fp32 += nq;
+        p->tiles.push_back(*tp);
+      }
     }
   }
   // flops: per tile class
@@ -793,11 +1003,30 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       long long tp = 0;
       for (size_t r = 0; r < t.rows.size(); ++r) {
         const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
-        tp += (long long)o->pair_nprim[t.rows[r]] * cum[cnt];
+        tp += (long long)o->pair_nprim[t.rows[r]] * (cum[t.col0(r) + cnt] - cum[t.col0(r)]);
       }
       nprimq += tp;
       const long long nq = t.row_prefix.back();
       flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
+    }
+  }
+  // primitive screening threshold per kernel class and precision: the dropped primitive
+  // quartets of one contracted quartet sum to at most prim_budget in its spherical block
+  std::map<std::tuple<int, int, int, int, int>, double> class_eps;
+  if (prim_budget > 0) {
+    std::map<std::tuple<int, int, int, int, int>, double> maxprod;
+    for (const Tile& t : p->tiles) {
+      int mr = 1, mc = 1;
+      for (int id : t.rows) mr = std::max(mr, o->pair_nprim[id]);
+      for (int id : t.cols) mc = std::max(mc, o->pair_nprim[id]);
+      auto key = std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32);
+      maxprod[key] = std::max(maxprod[key], (double)mr * mc);
+    }
+    for (auto& kv : maxprod) {
+      const int li = std::get<0>(kv.first), lj = std::get<1>(kv.first), lk = std::get<2>(kv.first),
+                ll = std::get<3>(kv.first);
+      const double amp = c2s_amp(li, p->sph) * c2s_amp(lj, p->sph) * c2s_amp(lk, p->sph) * c2s_amp(ll, p->sph);
+      class_eps[kv.first] = prim_budget / (kv.second * amp);
     }
   }
   // 3. chunks: greedy fill up to max_chunk doubles, splitting tiles at quartet boundaries
@@ -829,6 +1058,11 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       sg.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
       sg.expcutoff = ecut;
       sg.tile = ti;
+      sg.fp32 = t.fp32;
+      {
+        auto it = class_eps.find(std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32));
+        sg.prim_eps = it == class_eps.end() ? 0.0 : it->second;
+      }
       sg.t0 = q;
       sg.t1 = q + take;
       sg.nout = nout;
@@ -842,7 +1076,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
         long long pos = q;
         while (pos < q + take) {
           const long long rend = std::min(t.row_prefix[r + 1], q + take);
-          const long long c0 = pos - t.row_prefix[r], c1 = rend - t.row_prefix[r];
+          const long long c0 = t.col0(r) + pos - t.row_prefix[r], c1 = t.col0(r) + rend - t.row_prefix[r];
           fl += (double)o->pair_nprim[t.rows[r]] * (double)(t.cum_np[c1] - t.cum_np[c0]) * fpp;
           pos = rend;
           ++r;
@@ -868,6 +1102,10 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
     ok = cudaMalloc(&t.d_rows, sizeof(int) * t.rows.size()) == cudaSuccess &&
          cudaMalloc(&t.d_cols, sizeof(int) * t.cols.size()) == cudaSuccess &&
          cudaMalloc(&t.d_prefix, sizeof(long long) * t.row_prefix.size()) == cudaSuccess;
+    if (ok && !t.colstart.empty()) {
+      ok = cudaMalloc(&t.d_colstart, sizeof(int) * t.colstart.size()) == cudaSuccess;
+      if (ok) cudaMemcpy(t.d_colstart, t.colstart.data(), sizeof(int) * t.colstart.size(), cudaMemcpyHostToDevice);
+    }
     if (ok) {
       cudaMemcpy(t.d_rows, t.rows.data(), sizeof(int) * t.rows.size(), cudaMemcpyHostToDevice);
       cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
@@ -878,11 +1116,11 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
   // contiguous; each record carries its chunk-relative output offset)
   for (Chunk& ch : p->chunks) {
     std::vector<int> order;
-    std::map<std::tuple<int, int, int, int>, int> first;
+    std::map<std::tuple<int, int, int, int, int>, int> first;
     std::vector<std::vector<int>> members;
     for (int i = 0; i < (int)ch.pieces.size(); ++i) {
       const Segment& pc = ch.pieces[i];
-      auto key = std::make_tuple(pc.li, pc.lj, pc.lk, pc.ll);
+      auto key = std::make_tuple(pc.li, pc.lj, pc.lk, pc.ll, (int)pc.fp32);
       auto it = first.find(key);
       if (it == first.end()) {
         first[key] = (int)members.size();
@@ -903,6 +1141,8 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
       m.st = p0.st;
       m.expcutoff = p0.expcutoff;
       m.tile = -2;
+      m.fp32 = p0.fp32;
+      m.prim_eps = p0.prim_eps;
       m.rec0 = rec;
       m.out_off = 0;
       m.range0 = (int)p->ranges.size();
@@ -915,6 +1155,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
         g.prefix = t.d_prefix;
         g.nrows = (int)t.rows.size();
         g.pad = 0;
+        g.colstart = t.d_colstart;
         g.t0 = pc.t0;
         g.t1 = pc.t1;
         g.rec_off = m.nrec;
@@ -947,6 +1188,7 @@ int cintx_plan_int2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, in
   p->stats.max_chunk_doubles = maxc;
   p->stats.nprim_quartets = nprimq;
   p->stats.flops = flops;
+  p->stats.nquartets_fp32 = nq_fp32;
   {
     long long db = (long long)sizeof(QuartetRec) * max_recs;
     for (const Tile& t : p->tiles)

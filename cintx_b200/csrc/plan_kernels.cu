@@ -65,7 +65,7 @@ __global__ void gen_range_quartets(const GenRange* __restrict__ ranges, int nran
     }
     QuartetRec q;
     q.pij = g.rows[a];
-    q.pkl = g.cols[t - g.prefix[a]];
+    q.pkl = g.cols[(g.colstart ? g.colstart[a] : 0) + (t - g.prefix[a])];
     q.out = g.out_off + (r - g.rec_off) * g.nout;
     recs[r] = q;
   }

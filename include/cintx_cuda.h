@@ -126,6 +126,23 @@ CINTX_API int cintx_plan_int2e_screened(CintxPlan **plan, CINTOpt *opt, double c
 /* Device bytes held by an optimizer handle (pair and primitive-pair tables). */
 CINTX_API int64_t cintx_opt_device_bytes(CINTOpt *opt);
 
+/* The tuned sweep: the same quartet set as cintx_plan_int2e_screened, with two error-budgeted
+ * shortcuts built on primitive Schwarz factors q_ab = |c_a c_b| sqrt(max|(ab|ab)|) (computed on
+ * the device once per optimizer):
+ *   - primitive screening: a primitive quartet with q_ab q_cd below a per-class threshold is
+ *     skipped, the threshold chosen so the skipped terms of one block sum to <= prim_budget;
+ *   - mixed precision (spherical output only; classes with la+lb+lc+ld >= 4): a quartet runs
+ *     its recurrences and cartesian products in FP32 when its estimated FP32 error
+ *     64 * 2^-24 * (Qp amp)_ab (Qp amp)_cd * (c2s amplification) is below fp32_budget, where
+ *     Qp_ab = sum_ab q_ab and amp_ab = max over primitive pairs of (1 + |P - C| sqrt(2 a_ab))^(la+lb)
+ *     bounds the cancellation of the recurrences; roots, prefactors and the sum over primitives
+ *     stay FP64.
+ * Both are absolute error budgets per integral; fp32_budget <= 0 and prim_budget <= 0 give the
+ * FP64 plan. */
+CINTX_API int cintx_plan_int2e_screened_mixed(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
+                                              int64_t max_chunk_doubles, double fp32_budget,
+                                              double prim_budget);
+
 /* Plan statistics. */
 typedef struct {
   int64_t nquartets;        /* shell tuples in the plan */
@@ -134,6 +151,7 @@ typedef struct {
   int64_t max_chunk_doubles;/* largest chunk output */
   int64_t nprim_quartets;   /* primitive tuples surviving the pair screening */
   int64_t device_bytes;     /* device memory held by the plan (records, tile tables) */
+  int64_t nquartets_fp32;   /* quartets evaluated with FP32 recurrences (mixed plans) */
   double flops;             /* FP64 flops of the Rys path: per primitive quartet VRR 15*nroots*
                                (li+lj+1)(lk+ll+1), HRR 6*nroots per transfer step, products
                                3*nroots per cartesian element; per quartet the c2s stages */

@@ -190,6 +190,39 @@ def test_graph_replay_matches_direct_execution(cx):
         plan.close()
 
 
+def test_mixed_precision_plan_within_budget(cx, orc):
+    """Tuned plan with both shortcuts at 5e-11 each (primitive screening and FP32 recurrences
+    for quartets whose estimated FP32 error is below the budget): every integral of the checked
+    chunks stays within 1e-10 absolute of the FP64 evaluation (the tuned form's budget), and a
+    sample is also within that budget of the oracle."""
+    mol = M.mol40()
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened_mixed(opt, 1e-12, fp32_budget=5e-11, prim_budget=5e-11,
+                                      max_chunk_doubles=1 << 24)
+        st = plan.stats
+        assert 0 < st.nquartets_fp32 < st.nquartets
+        buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        worst = 0.0
+        rng = np.random.default_rng(8)
+        for c in sorted({0, st.nchunks // 2, st.nchunks - 1}):
+            plan.execute(buf.data_ptr(), chunk=c, stream=s)
+            torch.cuda.synchronize()
+            got = buf[:plan.chunk_size(c)].cpu().numpy()
+            quart = plan.chunk_quartets(c)
+            ref_plan = cx.Plan.shells(opt, cx.INT2E, quart, sph=True)
+            ref = ref_plan.execute_host(np.zeros(ref_plan.stats.nintegrals))
+            ref_plan.close()
+            worst = max(worst, float(np.abs(got - ref).max()))
+            offs = ref_plan.offsets
+            for k in rng.choice(len(quart), size=50, replace=False):
+                r, _ = orc.int2e(quart[k], mol)
+                assert np.abs(got[offs[k]:offs[k] + r.size] - r).max() <= 1e-10
+        assert worst <= 1e-10, worst
+        plan.close()
+
+
 def orc_block(mol, q):
     n = 1
     for s in q:
