@@ -58,7 +58,7 @@ REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cint_cpu_bench")
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="mol40_spd", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--error-chunks", type=int, default=4)
     ap.add_argument("--fp32-budget", type=float, default=FP32_BUDGET)
+    ap.add_argument("--no-autotune", action="store_true", help="tuned form without the launch-shape autotuner")
+    ap.add_argument("--e2e-chunk-doubles", type=int, default=1 << 24,
+                    help="chunk size of the end-to-end plan (copies of one chunk overlap the next chunk's kernels)")
     ap.add_argument("--prim-budget", type=float, default=PRIM_BUDGET)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -78,50 +81,74 @@ def parse():
 
 # ------------------------------------------------------------------ clocks
 class Clocks:
-    """nvidia-smi sampling every 200 ms while the timed region runs."""
+    """SM clock and clock-event reasons sampled every 5 ms through NVML (read-only queries) while
+    the timed region runs; the device is matched to the CUDA device by PCI bus id.  Without NVML
+    the line reports no samples and the reason."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index: int):
         self.index = index
+        self.samples = []
+        self.stop_flag = None
+        self.thread = None
         self.proc = None
-        self.path = None
+        self.err = None
+
+    def _handle(self, nv):
+        import torch
+        p = torch.cuda.get_device_properties(self.index)
+        bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        try:
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001 - any NVML failure means "no samples", never a crash
+            self.err = "nvml unavailable: %s" % e
+            return
+        self.stop_flag = threading.Event()
+
+        def run():
+            while not self.stop_flag.is_set():
+                try:
+                    self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
+                                         nv.nvmlDeviceGetCurrentClocksEventReasons(h),
+                                         nv.nvmlDeviceGetPowerUsage(h) / 1000.0))
+                except Exception:  # noqa: BLE001
+                    pass
+                self.stop_flag.wait(0.005)
+
+        self.nv = nv
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": [self.err or "no sampler"]}
+        self.stop_flag.set()
+        self.thread.join()
+        reasons = set()
+        for _, _, mask, _ in self.samples:
+            for name, const in self.REASONS:
+                if mask & getattr(self.nv, const):
+                    reasons.add(name)
+        sm = [x[0] for x in self.samples]
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "sm_min_mhz": min(sm) if sm else None,
+                "sm_max_mhz": max(x[1] for x in self.samples) if self.samples else None,
+                "power_w_median": statistics.median([x[3] for x in self.samples]) if self.samples else None,
+                "samples": len(sm), "sampler": "NVML every 5 ms", "reasons": sorted(reasons)}
 
 
 # ------------------------------------------------------------------ CPU baseline (libcint)
@@ -260,13 +287,23 @@ def fp64_peak(cx, torch):
     return best
 
 
-def timed_sweep(cx, torch, plan, mine, args, stream, local, world):
+def timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=False):
     """Warm-up, then exactly args.steps timed passes of `plan` over the rank's chunks (one CUDA
-    graph per pass unless --no-graph), L2 flushed between passes outside the events."""
+    graph per pass unless --no-graph), L2 flushed between passes outside the events.  With
+    tune, the plan's launch shapes are autotuned first on the rank's heaviest chunk."""
     import torch.distributed as dist
     st = plan.stats
     ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    tuning = None
+    if tune and mine:
+        t0 = time.perf_counter()
+        plan.autotune(ring.data_ptr(), chunk=-1, stream=stream.cuda_stream, reps=2)
+        lanes = {}
+        for c in mine:
+            for cl, n in zip(plan.segments(c)[0], plan.segment_lanes(c)):
+                lanes["(%d%d|%d%d)" % tuple(cl)] = int(n)
+        tuning = {"seconds": time.perf_counter() - t0, "lanes_per_quartet": dict(sorted(lanes.items()))}
     use_graph = not args.no_graph
     if use_graph:
         try:
@@ -307,7 +344,8 @@ def timed_sweep(cx, torch, plan, mine, args, stream, local, world):
     launches = cx.launch_count() - launches0
     clk = clocks.stop()
     ms = max_over_ranks(sum(step_ms), device="cuda") / args.steps
-    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": ring}
+    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": ring,
+            "tuning": tuning}
 
 
 def class_profile(torch, plan, mine, ring, stream):
@@ -389,7 +427,7 @@ def our_arm(args):
     stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
     torch.cuda.set_stream(stream)
 
-    main_run = timed_sweep(cx, torch, plan, mine, args, stream, local, world)
+    main_run = timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=tuned and not args.no_autotune)
     ms_per_step = main_run["ms"]
     value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
     plain = None
@@ -430,8 +468,10 @@ def our_arm(args):
     except Exception:
         pass
     form = ("tuned: primitive Schwarz screening (budget %g per integral), FP32 recurrences where the estimated "
-            "FP32 error is below %g, "
-            "graph-batched" % (args.prim_budget, args.fp32_budget)) if tuned else "plain FP64"
+            "FP32 error is below %g, %s, graph-batched" % (args.prim_budget, args.fp32_budget,
+                                                         "launch shapes autotuned per class" if not args.no_autotune
+                                                         else "default launch shapes")) if tuned else \
+        "plain FP64 (default launch shapes, libcint screening only)"
     line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (%s form)" % ("tuned" if tuned else "plain FP64"),
             "value": value, "unit": "Gint/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -456,36 +496,64 @@ def our_arm(args):
                               "gint_s": round(v["ints"] / (v["ms"] * 1e-3) / 1e9, 2), "quartets": v["quartets"]}
                           for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:16]},
             "profiled_step_ms": sum(v["ms"] for v in per_class.values())}
+    if main_run["tuning"] is not None:
+        line["autotune"] = main_run["tuning"]
     if plain is not None:
         line["plain_fp64"] = plain
         line["tuned_over_plain"] = value / plain["value"]
     if err is not None:
         line["error_vs_fp64"] = err
 
-    # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1)
+    # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1):
+    # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory
     if not args.no_e2e:
-        host = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, pin_memory=True).numpy()
-        e2e_times = []
+        e2e_chunk = args.e2e_chunk_doubles
+
+        def e2e_plan(o):
+            if tuned:
+                return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=args.fp32_budget, prim_budget=args.prim_budget,
+                                              max_chunk_doubles=e2e_chunk)
+            return cx.Plan.screened(o, SCHWARZ, sph=True, max_chunk_doubles=e2e_chunk)
+
+        host = torch.empty(max(st.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
+        phases = {"optimizer": [], "plan": [], "execute_d2h": []}
         h2d = d2h = 0
         for s in range(1 + max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             o2 = cx.Optimizer(mol.atm, mol.bas, mol.env)
-            p2 = make_plan(o2, tuned)
-            for c in mine:
-                p2.execute_host(host, chunk=c)
             t1 = time.perf_counter()
+            p2 = e2e_plan(o2)
+            if tuned and not args.no_autotune:
+                p2.use_tuned_shapes()  # shapes autotuned once in this process (before the timed sweep)
+            t2 = time.perf_counter()
+            if world == 1:
+                p2.execute_host(host)
+            else:
+                e2e_mine = chunks_of(assign_chunks([float(p2.segments(c)[2].sum()) for c in range(p2.stats.nchunks)],
+                                                   world), rank)
+                off = 0
+                for c in e2e_mine:
+                    p2.execute_host(host[off:], chunk=c)
+                    off += p2.chunk_size(c)
+            t3 = time.perf_counter()
             if s > 0:
-                e2e_times.append(t1 - t0)
-            h2d = o2.device_bytes + p2.stats.device_bytes + mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes
-            d2h = my_ints * 8
+                phases["optimizer"].append(t1 - t0)
+                phases["plan"].append(t2 - t1)
+                phases["execute_d2h"].append(t3 - t2)
+            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + p2.stats.device_bytes
+            d2h = (st.nintegrals if world == 1 else off) * 8
             p2.close()
             o2.close()
-        te = statistics.mean(e2e_times)
-        line["e2e"] = {"value": st.nintegrals / te / 1e9 if world == 1 else my_ints / te / 1e9 * world,
+        te = sum(statistics.mean(v) for v in phases.values())
+        line["e2e"] = {"value": st.nintegrals / te / 1e9 if world == 1 else d2h / 8 / te / 1e9 * world,
                        "unit": "Gint/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "seconds_per_step": te,
-                       "includes": "int2e_optimizer + screened plan (Schwarz pass) + execution + D2H of every chunk"}
+                       "phases_s": {k: statistics.mean(v) for k, v in phases.items()},
+                       "chunk_doubles": e2e_chunk,
+                       "includes": "int2e_optimizer from host atm/bas/env (pair tables, Schwarz passes) + screened "
+                                   "plan + evaluation + D2H of every integral into page-locked host memory "
+                                   "(copies overlapped with the next chunk's kernels)"}
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
         line["cpu_baseline"] = cpu_rate(mol, lambda n, seed: plan.sample_quartets(n, seed), st.nquartets,
                                         st.nintegrals, args.cpu_seconds, os.cpu_count() or 1)

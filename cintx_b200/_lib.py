@@ -72,6 +72,12 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute.restype = _i
     L.cintx_plan_execute_host.argtypes = [_vp, _i64, _dp]
     L.cintx_plan_execute_host.restype = _i
+    L.cintx_plan_autotune.argtypes = [_vp, _i64, ctypes.c_void_p, ctypes.c_void_p, _i]
+    L.cintx_plan_autotune.restype = _i
+    L.cintx_plan_use_tuned_shapes.argtypes = [_vp]
+    L.cintx_plan_use_tuned_shapes.restype = _i
+    L.cintx_plan_segment_lanes.argtypes = [_vp, _i64, _ip, _i]
+    L.cintx_plan_segment_lanes.restype = _i
     L.cintx_plan_destroy.argtypes = [_vp]
     L.cintx_plan_destroy.restype = None
     L.cintx_launch_count.restype = _i64
@@ -302,11 +308,35 @@ class Plan:
             _check(lib.cintx_plan_graph_build(self.handle, c.ctypes.data_as(_i64p), c.size,
                                               ctypes.c_void_p(out_ptr), nbranch))
 
+    def autotune(self, out_ptr: int, chunk: int = -1, stream: int = 0, reps: int = 2):
+        """Pick each kernel class's fastest launch shape by timing it on `chunk` (-1: each class
+        on its largest segment in the plan).  Synchronous; a captured graph is released and must
+        be built again."""
+        _check(lib.cintx_plan_autotune(self.handle, chunk, ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream), reps))
+
+    def use_tuned_shapes(self) -> int:
+        """Reuse the launch shapes autotuned earlier in this process; returns segments changed."""
+        n = lib.cintx_plan_use_tuned_shapes(self.handle)
+        if n < 0:
+            _check(1)
+        return n
+
+    def segment_lanes(self, chunk: int) -> np.ndarray:
+        n = lib.cintx_plan_segment_lanes(self.handle, chunk, None, 0)
+        out = np.zeros(max(n, 0), dtype=np.int32)
+        lib.cintx_plan_segment_lanes(self.handle, chunk, out.ctypes.data_as(_ip), n)
+        return out
+
     def graph_launch(self, stream: int = 0):
         _check(lib.cintx_plan_graph_launch(self.handle, ctypes.c_void_p(stream)))
 
     def execute_host(self, out: np.ndarray, chunk: int = -1):
-        assert out.dtype == np.float64 and out.flags.c_contiguous
+        """Evaluate one chunk (or all, chunks back to back) into host array `out`."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array")
+        need = self.stats.nintegrals if chunk < 0 else self.chunk_size(chunk)
+        if out.size < need:
+            raise ValueError("out holds %d doubles, the output needs %d" % (out.size, need))
         _check(lib.cintx_plan_execute_host(self.handle, chunk, out.ctypes.data_as(_dp)))
         return out
 

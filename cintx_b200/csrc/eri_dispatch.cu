@@ -7,7 +7,7 @@ namespace cintx {
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32,
-                         double prim_eps) {
+                         double prim_eps, int variant) {
   LaunchArgs a;
   a.recs = recs;
   a.nrec = nrec;
@@ -21,12 +21,21 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
   a.max_blocks = 0;
   a.fp32 = fp32;
   a.prim_eps = prim_eps;
+  a.variant = variant;
   return dispatch_eri(li, lj, lk, ll, sph, a);
 }
 
-bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph) {
+static_assert(kNumVariants == kLaunchVariants, "variant count differs between kernel and host headers");
+
+int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
+  if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  return pick_threads(li, lj, lk, ll, variant_acc(variant));
+}
+
+bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant) {
   LaunchArgs a{};
   a.query = 1;
+  a.variant = variant;
   return dispatch_eri(li, lj, lk, ll, sph, a) == cudaErrorNotSupported;
 }
 

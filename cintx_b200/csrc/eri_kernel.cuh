@@ -47,15 +47,22 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // Threads per quartet: smallest power of two keeping <= 24 accumulators per lane, capped by
 // the tuple count and by 256.
-__host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll) {
+// Lanes per quartet: the fewest (a power of two, at most twice the (j,k,l) tuple count) that
+// keep a lane's cartesian accumulators within `acc` doubles.
+__host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, int acc = 24) {
   const int ntup = ncart(lj) * ncart(lk) * ncart(ll);
   const int total = ntup * ncart(li);
   int s = 1;
-  while (s < 256 && (total + s - 1) / s > 24 && s * 2 <= ntup * 2) s *= 2;
+  while (s < 256 && (total + s - 1) / s > acc && s * 2 <= ntup * 2) s *= 2;
   return s;
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
+// Launch-shape variants the autotuner chooses between: the accumulator budget per lane
+// (variant 0 is the default shape, used by plans that are not autotuned).
+constexpr int kNumVariants = 3;
+__host__ __device__ constexpr int variant_acc(int v) { return v == 1 ? 48 : (v == 2 ? 12 : 24); }
+
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -63,7 +70,7 @@ struct EriShape {
   static constexpr int GSZ = NI * NJ * NK * NL;
   static constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
   static constexpr int NTUP = NFJ * NFK * NFL;
-  static constexpr int S = pick_threads(LI, LJ, LK, LL);
+  static constexpr int S = pick_threads(LI, LJ, LK, LL, ACC);
   static constexpr int TPT = (NTUP + S - 1) / S;
   static constexpr int MI = SPH && LI >= 2 ? 2 * LI + 1 : NFI;
   static constexpr int MJ = SPH && LJ >= 2 ? 2 * LJ + 1 : NFJ;
@@ -373,13 +380,14 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
   }
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R>::BLOCK, EriShape<LI, LJ, LK, LL, SPH, R>::MINB)
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC>::BLOCK,
+                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
                  double prim_eps) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];

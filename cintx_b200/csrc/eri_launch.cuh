@@ -20,6 +20,7 @@ struct LaunchArgs {
   int query = 0;   // 1: launch nothing; return cudaErrorNotSupported if the class needs scratch
   bool fp32 = false;  // FP32 recurrences and products (spherical output only)
   double prim_eps = 0;  // primitive Schwarz threshold (0: no primitive screening beyond libcint's)
+  int variant = 0;      // launch-shape variant (spherical FP64 classes; see variant_acc)
 };
 
 // Device scratch for classes whose transform buffers live in global memory: returns a buffer
@@ -34,11 +35,11 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 
 int device_sm_count();
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -80,8 +81,15 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
       constexpr int k = decltype(K)::value, l = decltype(L)::value;
       if constexpr (class_valid(LI, LJ, k, l)) {
         if (lk == k && ll == l) {
+          // variants that give the default lane count are not compiled separately
+          constexpr int s0 = pick_threads(LI, LJ, k, l, variant_acc(0));
+          constexpr int s1 = pick_threads(LI, LJ, k, l, variant_acc(1));
+          constexpr int s2 = pick_threads(LI, LJ, k, l, variant_acc(2));
           if (a.fp32) err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
-          else err = sph ? launch_eri<LI, LJ, k, l, true>(a) : launch_eri<LI, LJ, k, l, false>(a);
+          else if (!sph) err = launch_eri<LI, LJ, k, l, false>(a);
+          else if (a.variant == 1 && s1 != s0) err = launch_eri<LI, LJ, k, l, true, double, variant_acc(1)>(a);
+          else if (a.variant == 2 && s2 != s0) err = launch_eri<LI, LJ, k, l, true, double, variant_acc(2)>(a);
+          else err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }
     });

@@ -130,10 +130,14 @@ struct Oriented {
 double flops_per_prim_quartet(int li, int lj, int lk, int ll);
 double flops_c2s(int li, int lj, int lk, int ll, bool sph);
 
-bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph);
+bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant = 0);
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32 = false,
-                         double prim_eps = 0.0);
+                         double prim_eps = 0.0, int variant = 0);
+// Lanes per quartet of a launch-shape variant (0 = default shape); variants that do not apply
+// (cartesian or FP32 classes, unknown ids) report the default shape.
+int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
+constexpr int kLaunchVariants = 3;
 
 }  // namespace cintx

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <tuple>
@@ -50,6 +51,7 @@ struct Segment {
   int nranges = 0;
   bool fp32 = false;       // FP32 recurrences (mixed-precision plans)
   double prim_eps = 0;     // primitive Schwarz threshold (tuned plans)
+  int variant = 0;         // launch shape chosen by cintx_plan_autotune (0: default)
 };
 
 struct Chunk {
@@ -98,6 +100,9 @@ struct CintxPlan {
   double* d_stage = nullptr;
   long long stage_cap = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_done[2] = {nullptr, nullptr};
+  cudaEvent_t ev_free[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -126,6 +131,13 @@ void free_plan_device(CintxPlan* p) {
   p->events.clear();
   if (p->stream) cudaStreamDestroy(p->stream);
   p->stream = nullptr;
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+  p->copy_stream = nullptr;
+  for (int b = 0; b < 2; ++b) {
+    if (p->ev_done[b]) cudaEventDestroy(p->ev_done[b]);
+    if (p->ev_free[b]) cudaEventDestroy(p->ev_free[b]);
+    p->ev_done[b] = p->ev_free[b] = nullptr;
+  }
 }
 
 // Kernel class and strides for a quartet of oriented pairs (first pair is kernel (ij)).
@@ -365,7 +377,8 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
   for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
     const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
     cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
-                                 out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps);
+                                 out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps,
+                                 sg.variant);
     if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -426,31 +439,63 @@ int cintx_plan_execute_host(CintxPlan* p, int64_t chunk, double* out_host) {
     set_error(CINTX_STATUS_NULL_POINTER, "plan and out_host must not be NULL");
     return CINTX_STATUS_NULL_POINTER;
   }
+  if (chunk >= (int64_t)p->chunks.size()) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "chunk index out of range");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
   if (!p->stream && cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
     set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
     return CINTX_STATUS_EXECUTION_FAILED;
   }
+  if (!p->copy_stream && cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  for (int b = 0; b < 2; ++b) {
+    if ((!p->ev_done[b] && cudaEventCreateWithFlags(&p->ev_done[b], cudaEventDisableTiming) != cudaSuccess) ||
+        (!p->ev_free[b] && cudaEventCreateWithFlags(&p->ev_free[b], cudaEventDisableTiming) != cudaSuccess)) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaEventCreate failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+  }
   const int64_t c0 = chunk < 0 ? 0 : chunk, c1 = chunk < 0 ? (int64_t)p->chunks.size() : chunk + 1;
-  long long need = 0;
+  // two staging buffers when several chunks run: chunk c+1 is evaluated into one while chunk c
+  // is copied to the host from the other (copy stream), so the copies hide behind the kernels
+  const int nbuf = c1 - c0 > 1 ? 2 : 1;
+  long long need = 1;
   for (int64_t c = c0; c < c1; ++c) need = std::max(need, p->chunks[c].out_size);
-  if (need > p->stage_cap) {
+  if (need * nbuf > p->stage_cap) {
     if (p->d_stage) cudaFree(p->d_stage);
-    if (cudaMalloc(&p->d_stage, sizeof(double) * std::max<long long>(need, 1)) != cudaSuccess) {
+    if (cudaMalloc(&p->d_stage, sizeof(double) * need * nbuf) != cudaSuccess) {
       p->d_stage = nullptr;
       p->stage_cap = 0;
       set_error(CINTX_STATUS_ALLOCATION_FAILED, "device output staging allocation failed");
       return CINTX_STATUS_ALLOCATION_FAILED;
     }
-    p->stage_cap = need;
+    p->stage_cap = need * nbuf;
   }
-  for (int64_t c = c0; c < c1; ++c) {
-    int rc = cintx_plan_execute(p, c, p->d_stage, p->stream);
-    if (rc) return rc;
-    cudaMemcpyAsync(out_host, p->d_stage, sizeof(double) * p->chunks[c].out_size, cudaMemcpyDeviceToHost, p->stream);
+  long long hoff = 0;
+  int rc = CINTX_STATUS_SUCCESS;
+  for (int64_t c = c0; c < c1 && !rc; ++c) {
+    const int b = (int)((c - c0) % nbuf);
+    double* stage = p->d_stage + (size_t)b * need;
+    if (c - c0 >= nbuf) cudaStreamWaitEvent(p->stream, p->ev_free[b], 0);  // its previous copy is done
+    rc = cintx_plan_execute(p, c, stage, p->stream);
+    if (rc) break;
+    cudaEventRecord(p->ev_done[b], p->stream);
+    cudaStreamWaitEvent(p->copy_stream, p->ev_done[b], 0);
+    cudaMemcpyAsync(out_host + hoff, stage, sizeof(double) * p->chunks[c].out_size, cudaMemcpyDeviceToHost,
+                    p->copy_stream);
+    cudaEventRecord(p->ev_free[b], p->copy_stream);
+    hoff += p->chunks[c].out_size;
   }
-  cudaError_t e = cudaStreamSynchronize(p->stream);
-  if (e != cudaSuccess) {
-    set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("device execution failed: ") + cudaGetErrorString(e));
+  // drain both streams even after a failed launch, so no copy is left writing into out_host
+  cudaError_t e1 = cudaStreamSynchronize(p->stream);
+  cudaError_t e2 = cudaStreamSynchronize(p->copy_stream);
+  if (rc) return rc;
+  if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED,
+              std::string("device execution failed: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
     return CINTX_STATUS_EXECUTION_FAILED;
   }
   return CINTX_STATUS_SUCCESS;
@@ -563,6 +608,132 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
 // writing to out_dev.  Inside a chunk the kernel classes are independent (disjoint outputs)
 // and are spread over `nbranch` parallel branches by their flop estimate; chunks follow each
 // other because they share out_dev.
+// Launch shapes chosen by the autotuner, per device and class (li, lj, lk, ll, fp32): kept for
+// the life of the process so that later plans can reuse them (cintx_plan_use_tuned_shapes).
+static std::mutex g_tuned_mu;
+static std::map<std::tuple<int, int, int, int, int, int>, int> g_tuned;
+
+int cintx_plan_autotune(CintxPlan* p, int64_t chunk, double* out_dev, void* stream_, int reps) {
+  clear_error();
+  cudaStream_t stream;
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc = exec_prepare(p, out_dev, stream_, &stream, &ds, &ts);
+  if (rc) return rc;
+  if (chunk >= (int64_t)p->chunks.size()) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "chunk index out of range");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  reps = std::max(1, std::min(reps, 100));
+  // the segment each class is timed on: its first in `chunk`, or (chunk < 0) its largest in
+  // the plan, so that classes living in different chunks are all tuned
+  std::map<std::tuple<int, int, int, int, int>, std::pair<int64_t, int>> target;
+  for (int64_t c = chunk < 0 ? 0 : chunk; c < (chunk < 0 ? (int64_t)p->chunks.size() : chunk + 1); ++c)
+    for (int i = 0; i < (int)p->chunks[c].segs.size(); ++i) {
+      const Segment& sg = p->chunks[c].segs[i];
+      const auto key = std::make_tuple(sg.li, sg.lj, sg.lk, sg.ll, (int)sg.fp32);
+      auto it = target.find(key);
+      if (it == target.end() || (chunk < 0 && p->chunks[it->second.first].segs[it->second.second].nrec < sg.nrec))
+        target[key] = std::make_pair(c, i);
+    }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaEventCreate failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  // time every class segment of the chunk in each launch shape that gives a distinct lane
+  // count (and needs device scratch only if the default shape does, so graphs stay possible)
+  std::map<std::tuple<int, int, int, int, int>, int> best;
+  for (const auto& tg : target) {
+    const auto& key = tg.first;
+    const Segment& sg0 = p->chunks[tg.second.first].segs[tg.second.second];
+    const bool scratch0 = class_needs_scratch(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, 0);
+    std::vector<int> lanes_seen;
+    double best_ms = 1e300;
+    int best_v = 0;
+    for (int v = 0; v < kLaunchVariants && !rc; ++v) {
+      const int lanes = variant_lanes(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, sg0.fp32, v);
+      if (std::find(lanes_seen.begin(), lanes_seen.end(), lanes) != lanes_seen.end()) continue;
+      lanes_seen.push_back(lanes);
+      if (!scratch0 && class_needs_scratch(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, v)) continue;
+      Segment sg = sg0;
+      sg.variant = v;
+      if ((rc = run_segment(p, sg, out_dev, stream, ds, ts))) break;  // warm-up
+      cudaEventRecord(e0, stream);
+      for (int r = 0; r < reps && !rc; ++r) rc = run_segment(p, sg, out_dev, stream, ds, ts);
+      cudaEventRecord(e1, stream);
+      if (rc) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        set_error(CINTX_STATUS_EXECUTION_FAILED, "device execution failed during autotuning");
+        rc = CINTX_STATUS_EXECUTION_FAILED;
+        break;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_v = v;
+      }
+    }
+    if (rc) break;
+    best[key] = best_v;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    for (const auto& kv : best)
+      g_tuned[std::make_tuple(dev, std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                              std::get<3>(kv.first), std::get<4>(kv.first))] = kv.second;
+  }
+  for (Chunk& ch : p->chunks)
+    for (Segment& sg : ch.segs) {
+      auto it = best.find(std::make_tuple(sg.li, sg.lj, sg.lk, sg.ll, (int)sg.fp32));
+      if (it != best.end()) sg.variant = it->second;
+    }
+  if (p->gexec) {  // the captured graph holds the old launch shapes
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_use_tuned_shapes(CintxPlan* p) {
+  clear_error();
+  if (!p) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
+    return -1;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int applied = 0;
+  std::lock_guard<std::mutex> lk(g_tuned_mu);
+  for (Chunk& ch : p->chunks)
+    for (Segment& sg : ch.segs) {
+      auto it = g_tuned.find(std::make_tuple(dev, sg.li, sg.lj, sg.lk, sg.ll, (int)sg.fp32));
+      if (it != g_tuned.end()) {
+        sg.variant = it->second;
+        ++applied;
+      }
+    }
+  if (applied && p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  return applied;
+}
+
+int cintx_plan_segment_lanes(const CintxPlan* p, int64_t chunk, int* lanes, int cap) {
+  if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return -1;
+  const std::vector<Segment>& segs = p->chunks[chunk].segs;
+  for (int i = 0; i < (int)segs.size() && i < cap && lanes; ++i)
+    lanes[i] = variant_lanes(segs[i].li, segs[i].lj, segs[i].lk, segs[i].ll, p->sph, segs[i].fp32, segs[i].variant);
+  return (int)segs.size();
+}
+
 int cintx_plan_graph_build(CintxPlan* p, const int64_t* chunks, int64_t n, double* out_dev, int nbranch) {
   clear_error();
   if (!p || !out_dev) {
@@ -579,7 +750,7 @@ int cintx_plan_graph_build(CintxPlan* p, const int64_t* chunks, int64_t n, doubl
       return CINTX_STATUS_INVALID_INPUT;
     }
     for (const Segment& sg : p->chunks[c].segs)
-      if (class_needs_scratch(sg.li, sg.lj, sg.lk, sg.ll, p->sph)) {
+      if (class_needs_scratch(sg.li, sg.lj, sg.lk, sg.ll, p->sph, sg.variant)) {
         set_error(CINTX_STATUS_UNSUPPORTED_API, "plan contains classes with device scratch; use cintx_plan_execute");
         return CINTX_STATUS_UNSUPPORTED_API;
       }

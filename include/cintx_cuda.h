@@ -184,8 +184,25 @@ CINTX_API int cintx_plan_graph_build(CintxPlan *plan, const int64_t *chunks, int
                                      int nbranch);
 /* Launches the captured graph on `stream` (asynchronous). */
 CINTX_API int cintx_plan_graph_launch(CintxPlan *plan, void *stream);
-/* Same, end to end: device output staged through a device ring and copied to host memory
- * out_host (at least chunk size; all-chunk runs overwrite it per chunk).  Synchronous. */
+/* Autotuner: times every kernel class of chunk `chunk` (chunk < 0: every class of the plan, each
+ * on the chunk where it has the most quartets; reps runs after one warm-up, CUDA events on
+ * `stream`, output into out_dev of max_chunk_doubles) in each launch shape (lanes per quartet,
+ * hence quartets per block) that gives a distinct shape, and keeps the fastest per class for
+ * every chunk of the plan.  Synchronous.  A graph captured earlier is released: capture again
+ * after tuning. */
+CINTX_API int cintx_plan_autotune(CintxPlan *plan, int64_t chunk, double *out_dev, void *stream, int reps);
+/* Applies the launch shapes the autotuner chose earlier in this process on the current device
+ * (any plan) to this plan's matching classes; returns the number of segments changed (or -1).
+ * A graph captured earlier is released when anything changed. */
+CINTX_API int cintx_plan_use_tuned_shapes(CintxPlan *plan);
+/* Lanes per quartet of each segment of a chunk (as chosen by the autotuner, or the default
+ * shape).  Returns the segment count (or -1). */
+CINTX_API int cintx_plan_segment_lanes(const CintxPlan *plan, int64_t chunk, int *lanes, int cap);
+/* End to end: evaluates one chunk (chunk >= 0) or every chunk (chunk < 0) into device staging
+ * buffers and copies the output to host memory out_host, chunks back to back (out_host holds the
+ * chunk's size, or the plan's nintegrals for chunk < 0).  With several chunks the copy of chunk c
+ * runs on a second stream while chunk c+1 is evaluated (two staging buffers); page-locked
+ * out_host lets the copies overlap.  Synchronous. */
 CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);
 CINTX_API void cintx_plan_destroy(CintxPlan *plan);
 

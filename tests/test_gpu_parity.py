@@ -170,6 +170,65 @@ def test_screened_plan_mol40(cx, orc):
         plan.close()
 
 
+def test_execute_host_all_chunks_back_to_back(cx):
+    """The pipelined host path (two staging buffers, copies on a second stream) returns every
+    chunk back to back, bit-identical to the device path chunk by chunk."""
+    mol = M.mol40()
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 23)
+        st = plan.stats
+        assert st.nchunks >= 3
+        host = torch.empty(st.nintegrals, dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = np.nan
+        plan.execute_host(host)
+        buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        off = 0
+        for c in range(st.nchunks):
+            n = plan.chunk_size(c)
+            plan.execute(buf.data_ptr(), chunk=c, stream=s)
+            torch.cuda.synchronize()
+            assert np.array_equal(host[off:off + n], buf[:n].cpu().numpy()), c
+            off += n
+        assert off == st.nintegrals
+        with pytest.raises(ValueError):
+            plan.execute_host(np.zeros(st.nintegrals - 1))
+        plan.close()
+
+
+def test_autotuned_launch_shapes_give_the_same_integrals(cx):
+    """The autotuner may change lanes per quartet class by class; every chunk's output stays
+    within the parity tolerance of the default shapes, the choice is reported per segment, and a
+    second plan picks the cached shapes up."""
+    mol = M.mol40()
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 23)
+        st = plan.stats
+        s = torch.cuda.current_stream().cuda_stream
+        ref = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        got = torch.empty_like(ref)
+        default_lanes = [plan.segment_lanes(c) for c in range(st.nchunks)]
+        refs = []
+        for c in range(st.nchunks):
+            plan.execute(ref.data_ptr(), chunk=c, stream=s)
+            torch.cuda.synchronize()
+            refs.append(ref[:plan.chunk_size(c)].cpu().numpy())
+        plan.autotune(got.data_ptr(), chunk=0, stream=s, reps=1)
+        tuned_lanes = [plan.segment_lanes(c) for c in range(st.nchunks)]
+        assert all(len(a) == len(b) and (b > 0).all() for a, b in zip(default_lanes, tuned_lanes))
+        for c in range(st.nchunks):
+            plan.execute(got.data_ptr(), chunk=c, stream=s)
+            torch.cuda.synchronize()
+            assert close(got[:plan.chunk_size(c)].cpu().numpy(), refs[c]), c
+        other = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 23)
+        assert other.use_tuned_shapes() > 0
+        assert all(np.array_equal(other.segment_lanes(c), tuned_lanes[c]) for c in range(st.nchunks))
+        other.close()
+        plan.close()
+
+
 def test_graph_replay_matches_direct_execution(cx):
     mol = M.mol40()
     import torch
