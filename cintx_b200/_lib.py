@@ -93,6 +93,15 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_graph_launch.restype = _i
     L.cintx_opt_device_bytes.argtypes = [_vp]
     L.cintx_opt_device_bytes.restype = _i64
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.cintx_rysnet_samples.argtypes = [_i64, _i, _i, ctypes.c_uint64, _fp, _fp, _ip, _dp]
+    L.cintx_rysnet_samples.restype = _i
+    L.cintx_rysnet_loss_grad.argtypes = [_fp, _fp, _fp, _ip, _i64, _fp, _dp]
+    L.cintx_rysnet_loss_grad.restype = _i
+    L.cintx_rysnet_train.argtypes = [_fp, _i64, _i, _i, _i, _i, ctypes.c_float, ctypes.c_uint64, _dp]
+    L.cintx_rysnet_train.restype = _i
+    L.cintx_rys_learned_batch.argtypes = [_fp, _i, _dp, _i64, _i, _dp, _ip, _ip]
+    L.cintx_rys_learned_batch.restype = _i
     L.cintx_fp64_fma_probe.argtypes = [_i, _i, _i, _vp, _vp]
     L.cintx_fp64_fma_probe.restype = _i
     return L
@@ -350,3 +359,72 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+_fp32p = ctypes.POINTER(ctypes.c_float)
+
+
+class RysNet:
+    """Learned Rys-root initializer (include/cintx_cuda.h, cintx_rysnet_*): an FP32 MLP trained
+    on the device from the table path, whose guess an FP64 refinement turns into roots and
+    weights at full accuracy (table-path fallback where the refinement fails its checks)."""
+
+    NPARAM = 5522
+    SHAPES = [(64, 2), (64,), (64, 64), (64,), (18, 64), (18,)]
+
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0):
+        self.params = np.ascontiguousarray(params if params is not None else self.init(seed), dtype=np.float32)
+        assert self.params.size == self.NPARAM
+
+    @classmethod
+    def init(cls, seed: int = 0) -> np.ndarray:
+        """Glorot-uniform weights, zero biases."""
+        rng = np.random.default_rng(seed)
+        parts = []
+        for shp in cls.SHAPES:
+            if len(shp) == 2:
+                lim = np.sqrt(6.0 / (shp[0] + shp[1]))
+                parts.append(rng.uniform(-lim, lim, size=shp).ravel())
+            else:
+                parts.append(np.zeros(shp))
+        return np.concatenate(parts).astype(np.float32)
+
+    @staticmethod
+    def samples(count: int, n_lo: int = 5, n_hi: int = 9, seed: int = 0):
+        feat = np.zeros((count, 2), dtype=np.float32)
+        tgt = np.zeros((count, 18), dtype=np.float32)
+        nr = np.zeros(count, dtype=np.int32)
+        x = np.zeros(count)
+        _check(lib.cintx_rysnet_samples(count, n_lo, n_hi, seed, feat.ctypes.data_as(_fp32p),
+                                        tgt.ctypes.data_as(_fp32p), nr.ctypes.data_as(_ip), x.ctypes.data_as(_dp)))
+        return feat, tgt, nr, x
+
+    def loss_grad(self, feat, tgt, nroots):
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        tgt = np.ascontiguousarray(tgt, dtype=np.float32)
+        nr = np.ascontiguousarray(nroots, dtype=np.int32)
+        grad = np.zeros(self.NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        _check(lib.cintx_rysnet_loss_grad(self.params.ctypes.data_as(_fp32p), feat.ctypes.data_as(_fp32p),
+                                          tgt.ctypes.data_as(_fp32p), nr.ctypes.data_as(_ip), nr.size,
+                                          grad.ctypes.data_as(_fp32p), ctypes.byref(loss)))
+        return loss.value, grad
+
+    def train(self, nsamples: int = 5_000_000, n_lo: int = 5, n_hi: int = 9, epochs: int = 20,
+              batch: int = 16384, lr: float = 3e-3, seed: int = 1) -> np.ndarray:
+        hist = np.zeros(epochs)
+        _check(lib.cintx_rysnet_train(self.params.ctypes.data_as(_fp32p), nsamples, n_lo, n_hi, epochs, batch,
+                                      lr, seed, hist.ctypes.data_as(_dp)))
+        return hist
+
+    def roots(self, n: int, x, mode: int = 0):
+        """(t2, w, status, iters) for order n at points x; mode 0 network + refinement, 1 the
+        refinement from the x = 0 roots (no network), 2 the network's guess unrefined."""
+        x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        out = np.zeros((x.size, 2 * n))
+        st = np.zeros(x.size, dtype=np.int32)
+        it = np.zeros(x.size, dtype=np.int32)
+        _check(lib.cintx_rys_learned_batch(self.params.ctypes.data_as(_fp32p), n, x.ctypes.data_as(_dp), x.size,
+                                           mode, out.ctypes.data_as(_dp), st.ctypes.data_as(_ip),
+                                           it.ctypes.data_as(_ip)))
+        return out[:, :n], out[:, n:], st, it

@@ -232,6 +232,46 @@ CINTX_API void cintx_plan_destroy(CintxPlan *plan);
 CINTX_API int cintx_int2e_noalloc(double *out_dev, const int *shls, int64_t n, int sph, const int *atm,
                                   int natm, const int *bas, int nbas, const double *env, void *stream);
 
+/* ---- learned Rys-root initializer (RysNet) ------------------------------------------------ */
+
+/* The plain path these replace for a caller that opts in is CINTrys_roots
+ * (libcint-master/src/rys_roots.c:57; cintx-cubecl math/rys.rs).  RysNet is an MLP in FP32
+ * (inputs: nroots and log x; two hidden layers of 64 SiLU units; 18 outputs read as logit(t_i^2)
+ * for outputs 0..8 and log(w_i) for 9..17) whose CINTX_RYSNET_NPARAM parameters are, in order:
+ * W1[64][2], b1[64], W2[64][64] (row = output), b2[64], W3[18][64], b3[18]. */
+#define CINTX_RYSNET_NPARAM 5522
+
+/* count training samples drawn on the device (seeded): nroots uniform in [n_lo, n_hi], x
+ * log-uniform in [1e-7, 50] with probability 0.7 else uniform in [50, 3000], redrawn
+ * log-uniformly below the table range where it is reached.  feat[2*count] network inputs,
+ * tgt[18*count] targets from the table path (unused outputs 0), nroots[count], x[count] (x may be
+ * NULL).  Host arrays; synchronous. */
+CINTX_API int cintx_rysnet_samples(int64_t count, int n_lo, int n_hi, uint64_t seed, float *feat, float *tgt,
+                                   int *nroots, double *x);
+/* One forward and backward pass of the device training kernel over count samples (host arrays
+ * as produced by cintx_rysnet_samples): loss = mean over samples of the squared error of the
+ * sample's 2*nroots used outputs divided by 2*nroots, and its gradient grad[CINTX_RYSNET_NPARAM]
+ * with respect to params.  Synchronous. */
+CINTX_API int cintx_rysnet_loss_grad(const float *params, const float *feat, const float *tgt, const int *nroots,
+                                     int64_t count, float *grad, double *loss);
+/* Trains params (in: initial values, out: trained) on the device: nsamples samples as above,
+ * epochs passes of Adam (beta 0.9/0.999, cosine decay of lr to 1%) over minibatches of `batch`
+ * (a multiple of 128); loss_per_epoch[epochs] (may be NULL) receives each epoch's mean loss.
+ * Synchronous. */
+CINTX_API int cintx_rysnet_train(float *params, int64_t nsamples, int n_lo, int n_hi, int epochs, int batch,
+                                 float lr, uint64_t seed, double *loss_per_epoch);
+/* Rys roots t^2 and weights of order nroots (1..9) at count points x, in cintx_rys_t2_batch's
+ * layout t2w[p*2*nroots + f] (roots first), from the network's guess (mode 0; params on the
+ * host) or from the x = 0 roots (mode 1: the same refinement without the network), refined in
+ * FP64 (Stieltjes recurrence of the measure's 64-node discretisation, at most 8 Newton steps
+ * with the Aberth correction on the orthogonal polynomial, roots sorted and checked distinct
+ * and inside (0, 1), Christoffel weights); mode 2 returns the network's guess unrefined
+ * (status 3), for judging it against the table path.  status[p]: 0 refined, 1 the refinement
+ * failed its checks and the table path supplied the values (fallback), 2 x beyond the table range
+ * (closed form).  iters[p]: Newton steps of the slowest root.  Synchronous. */
+CINTX_API int cintx_rys_learned_batch(const float *params, int nroots, const double *x, int64_t count, int mode,
+                                      double *t2w, int *status, int *iters);
+
 /* FP64 FMA throughput probe (measurement only): blocks x threads threads each run
  * iters*16*8 FMAs and write one double to out_dev[blocks*threads].  Asynchronous on stream. */
 CINTX_API int cintx_fp64_fma_probe(int blocks, int threads, int iters, double *out_dev, void *stream);
