@@ -60,6 +60,10 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_int2e_screened.restype = _i
     L.cintx_plan_int2e_screened_mixed.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64, _d, _d]
     L.cintx_plan_int2e_screened_mixed.restype = _i
+    L.cintx_optimizer_pair_shells.argtypes = [ctypes.POINTER(_vp), _ip, _i, _ip, _i, _dp, _i]
+    L.cintx_optimizer_pair_shells.restype = _i
+    L.cintx_plan_int3c2e_screened.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64, _i]
+    L.cintx_plan_int3c2e_screened.restype = _i
     L.cintx_plan_stats.argtypes = [_vp, ctypes.POINTER(PlanStats)]
     L.cintx_plan_stats.restype = _i
     L.cintx_plan_chunk_size.argtypes = [_vp, _i64]
@@ -203,12 +207,17 @@ class Optimizer:
 
     _makers = {0: "int2e_optimizer", 1: "int3c2e_optimizer", 2: "int2c2e_optimizer"}
 
-    def __init__(self, atm, bas, env, family: int = 0):
+    def __init__(self, atm, bas, env, family: int = 0, pair_shells: int | None = None):
+        """pair_shells: build shell pairs only among the first pair_shells shells (orbital shells
+        of a density-fitting basis; cintx_optimizer_pair_shells)."""
         self.atm, self.bas, self.env = _arrs(atm, bas, env)
         self.handle = _vp()
-        getattr(lib, self._makers[family])(ctypes.byref(self.handle), self.atm.ctypes.data_as(_ip),
-                                           self.atm.shape[0], self.bas.ctypes.data_as(_ip),
-                                           self.bas.shape[0], self.env.ctypes.data_as(_dp))
+        args = (ctypes.byref(self.handle), self.atm.ctypes.data_as(_ip), self.atm.shape[0],
+                self.bas.ctypes.data_as(_ip), self.bas.shape[0], self.env.ctypes.data_as(_dp))
+        if pair_shells is None:
+            getattr(lib, self._makers[family])(*args)
+        else:
+            lib.cintx_optimizer_pair_shells(*args, int(pair_shells))
         if not self.handle:
             raise CintxError(*last_error())
 
@@ -270,6 +279,16 @@ class Plan:
         _check(lib.cintx_plan_int2e_screened_mixed(ctypes.byref(h), opt.handle, float(cutoff), 1,
                                                    int(max_chunk_doubles), float(fp32_budget),
                                                    float(prim_budget)))
+        return cls(h, opt)
+
+    @classmethod
+    def screened_3c(cls, opt: Optimizer, norb: int, cutoff: float = 1e-12, sph: bool = True,
+                    max_chunk_doubles: int = 1 << 28):
+        """Density-fitting sweep: (ab|k) over orbital pairs a >= b < norb and auxiliary shells
+        k >= norb with Schwarz bound >= cutoff (cintx_plan_int3c2e_screened)."""
+        h = _vp()
+        _check(lib.cintx_plan_int3c2e_screened(ctypes.byref(h), opt.handle, float(cutoff), int(sph),
+                                               int(max_chunk_doubles), int(norb)))
         return cls(h, opt)
 
     @property

@@ -53,7 +53,7 @@ struct __align__(16) GenRange {
   const int* cols;
   const long long* prefix;
   int nrows;
-  int pad;
+  int swap;  // nonzero: the column pair is the kernel's first pair (pij)
   long long t0, t1;
   long long rec_off;
   long long out_off;

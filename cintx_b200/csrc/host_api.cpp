@@ -330,15 +330,21 @@ static void free_opt_device(Opt* o) {
   o->d_prims = nullptr;
 }
 
-int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env) {
+int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env, int npair_shells) {
   int rc = load_basis(o->basis, atm, natm, bas, nbas, env);
   if (rc) return rc;
+  if (npair_shells > nbas) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "npair_shells exceeds nbas");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
   DeviceState* ds;
   if ((rc = device_state(&ds))) return rc;
   const Basis& B = o->basis;
   o->build_cutoff = expcutoff_2e(B.env.data());
   const int nv = B.nvirt;
-  o->npairs = nv * (nv + 1) / 2;
+  const int npv = npair_shells < 0 || npair_shells == B.nbas ? nv : B.sh[npair_shells].vbase;
+  o->npv = npv;
+  o->npairs = npv * (npv + 1) / 2;
   const int ntot = o->npairs + nv;
   std::vector<ShellPair> sps(ntot);
   std::vector<PrimPair> prims;
@@ -351,7 +357,7 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
   o->h_prim_a.clear();
   o->h_prim_b.clear();
   PairHost ph;
-  for (int u = 0; u < nv; ++u) {
+  for (int u = 0; u < npv; ++u) {
     for (int v = 0; v <= u; ++v) {
       const int lu = B.sh[B.vshell[u]].l, lv = B.sh[B.vshell[v]].l;
       const int a = lu >= lv ? u : v, b = lu >= lv ? v : u;
@@ -410,13 +416,14 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
   return CINTX_STATUS_SUCCESS;
 }
 
-static void make_optimizer(CINTOpt** opt, int* atm, int natm, int* bas, int nbas, double* env) {
+static void make_optimizer(CINTOpt** opt, const int* atm, int natm, const int* bas, int nbas, const double* env,
+                           int npair_shells = -1) {
   if (!opt) return;
   *opt = nullptr;
   clear_error();
   Opt* o = new Opt();
   o->magic = Opt::kMagic;
-  if (build_opt(o, atm, natm, bas, nbas, env) != CINTX_STATUS_SUCCESS) {
+  if (build_opt(o, atm, natm, bas, nbas, env, npair_shells) != CINTX_STATUS_SUCCESS) {
     free_opt_device(o);
     o->magic = 0;
     delete o;
@@ -713,6 +720,15 @@ void int3c2e_optimizer(CINTOpt** opt, int* atm, int natm, int* bas, int nbas, do
 }
 void int2c2e_optimizer(CINTOpt** opt, int* atm, int natm, int* bas, int nbas, double* env) {
   make_optimizer(opt, atm, natm, bas, nbas, env);
+}
+int cintx_optimizer_pair_shells(CINTOpt** opt, const int* atm, int natm, const int* bas, int nbas, const double* env,
+                                int npair_shells) {
+  if (!opt || npair_shells < 1 || npair_shells > nbas) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "cintx_optimizer_pair_shells: bad arguments");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  make_optimizer(opt, atm, natm, bas, nbas, env, npair_shells);
+  return *opt ? CINTX_STATUS_SUCCESS : cintx_cuda_last_error_code();
 }
 
 void CINTdel_optimizer(CINTOpt** opt) {

@@ -71,6 +71,7 @@ struct Opt {
   double build_cutoff = 0;
   int device = -1;
   int npairs = 0;             // regular pairs; unit pair of v is npairs + v
+  int npv = 0;                // virtual shells u < npv have their pairs (u, v <= u) stored
   std::vector<int> pair_a, pair_b, pair_la, pair_lb, pair_nprim;
   std::vector<double> pair_min_cce;
   ShellPair* d_pairs = nullptr;
@@ -97,7 +98,9 @@ Opt* as_opt(CINTOpt* o);
 // Computes every stored primitive pair's Schwarz factor q (cartesian primitive diagonals on the
 // device), sorts each shell pair's primitive pairs by decreasing q and re-uploads them.
 int compute_prim_schwarz(Opt* o);
-int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env);
+// npair_shells < 0: pairs of all shells; otherwise only pairs among the first npair_shells shells
+// (unit pairs are built for every shell).
+int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env, int npair_shells = -1);
 
 // Per-device constants (Rys table) and per-thread scratch.
 struct DeviceState {

@@ -52,6 +52,7 @@ struct Segment {
   bool fp32 = false;       // FP32 recurrences (mixed-precision plans)
   double prim_eps = 0;     // primitive Schwarz threshold (tuned plans)
   int variant = 0;         // launch shape chosen by cintx_plan_autotune (0: default)
+  bool swap = false;       // screened: the tile's records are (col, row) pairs
 };
 
 struct Chunk {
@@ -69,6 +70,8 @@ struct Tile {
   std::vector<long long> cum_np;        // prefix of primitive-pair counts over cols
   std::vector<int> colstart;            // per row: first column (empty: 0 for every row)
   bool fp32 = false;                    // evaluated with FP32 recurrences
+  bool swap = false;                    // records take (pij, pkl) = (col, row): the kernel's first pair is the col
+  OutStrides st{};                      // output strides of the kernel's axes
   int* d_rows = nullptr;
   int* d_cols = nullptr;
   long long* d_prefix = nullptr;
@@ -255,6 +258,13 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
                 x_first = (o->pair_a[id] == x);
               }
             };
+            if ((v[0] >= 0 && v[1] >= 0 && std::max(v[0], v[1]) >= o->npv) ||
+                (v[2] >= 0 && v[3] >= 0 && std::max(v[2], v[3]) >= o->npv)) {
+              delete p;
+              set_error(CINTX_STATUS_INVALID_INPUT, "tuple " + std::to_string(q) +
+                                                        " needs a shell pair this optimizer does not hold");
+              return CINTX_STATUS_INVALID_INPUT;
+            }
             int id1, id2;
             bool f1, f2;
             pair_of(v[0], v[1], id1, f1);
@@ -537,10 +547,11 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
         const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
         const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
         const Basis& B = o->basis;
+        // unit pairs (3-centre sweeps) have no second shell: -1
         quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
-        quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
+        quartets[k * 4 + 1] = o->pair_b[pa] < 0 ? -1 : B.vshell[o->pair_b[pa]];
         quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
-        quartets[k * 4 + 3] = B.vshell[o->pair_b[pb]];
+        quartets[k * 4 + 3] = o->pair_b[pb] < 0 ? -1 : B.vshell[o->pair_b[pb]];
       }
     }
   }
@@ -588,10 +599,11 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
       const long long q = g - tp[ti];
       const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
       const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
+      // unit pairs (3-centre sweeps) have no second shell: -1
       quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
-      quartets[k * 4 + 1] = B.vshell[o->pair_b[pa]];
+      quartets[k * 4 + 1] = o->pair_b[pa] < 0 ? -1 : B.vshell[o->pair_b[pa]];
       quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
-      quartets[k * 4 + 3] = B.vshell[o->pair_b[pb]];
+      quartets[k * 4 + 3] = o->pair_b[pb] < 0 ? -1 : B.vshell[o->pair_b[pb]];
     }
   } else {
     const long long total = (long long)p->h_tuples.size() / 4;
@@ -1010,6 +1022,220 @@ static double c2s_amp(int l, bool sph) {
   return sph && l >= 2 ? amp[std::min(l, 4)] : 1.0;
 }
 
+// Shared tail of the screened planners: flop model, primitive-screening thresholds, chunking at
+// quartet boundaries, per-class merged segments and device upload.  The tiles of p are complete
+// (rows, cols, row_prefix, cum_np, kernel class, strides, swap).
+static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk, double prim_budget,
+                           long long nq_total, long long nint_total, long long nq_fp32, CintxPlan** plan) {
+  long long nprimq = 0;
+  double flops = 0;
+  // flops: per tile class
+  {
+    // recompute nprim-weighted flops per tile
+    for (const Tile& t : p->tiles) {
+      std::vector<long long> cum(t.cols.size() + 1, 0);
+      for (size_t c = 0; c < t.cols.size(); ++c) cum[c + 1] = cum[c] + o->pair_nprim[t.cols[c]];
+      long long tp = 0;
+      for (size_t r = 0; r < t.rows.size(); ++r) {
+        const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
+        tp += (long long)o->pair_nprim[t.rows[r]] * (cum[t.col0(r) + cnt] - cum[t.col0(r)]);
+      }
+      nprimq += tp;
+      const long long nq = t.row_prefix.back();
+      flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
+    }
+  }
+  // primitive screening threshold per kernel class and precision: the dropped primitive
+  // quartets of one contracted quartet sum to at most prim_budget in its spherical block
+  std::map<std::tuple<int, int, int, int, int>, double> class_eps;
+  if (prim_budget > 0) {
+    std::map<std::tuple<int, int, int, int, int>, double> maxprod;
+    for (const Tile& t : p->tiles) {
+      int mr = 1, mc = 1;
+      for (int id : t.rows) mr = std::max(mr, o->pair_nprim[id]);
+      for (int id : t.cols) mc = std::max(mc, o->pair_nprim[id]);
+      auto key = std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32);
+      maxprod[key] = std::max(maxprod[key], (double)mr * mc);
+    }
+    for (auto& kv : maxprod) {
+      const int li = std::get<0>(kv.first), lj = std::get<1>(kv.first), lk = std::get<2>(kv.first),
+                ll = std::get<3>(kv.first);
+      const double amp = c2s_amp(li, p->sph) * c2s_amp(lj, p->sph) * c2s_amp(lk, p->sph) * c2s_amp(ll, p->sph);
+      class_eps[kv.first] = prim_budget / (kv.second * amp);
+    }
+  }
+  // 3. chunks: greedy fill up to max_chunk doubles, splitting tiles at quartet boundaries
+  Chunk cur;
+  long long max_recs = 0;
+  for (int ti = 0; ti < (int)p->tiles.size(); ++ti) {
+    const Tile& t = p->tiles[ti];
+    const long long nq = t.row_prefix.back();
+    const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
+                           nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
+    long long q = 0;
+    while (q < nq) {
+      long long room = (max_chunk - cur.out_size) / nout;
+      if (room <= 0) {
+        if (cur.pieces.empty()) room = 1;  // a single block larger than the chunk limit
+        else {
+          p->chunks.push_back(cur);
+          max_recs = std::max(max_recs, cur.nrec);
+          cur = Chunk();
+          continue;
+        }
+      }
+      const long long take = std::min(room, nq - q);
+      Segment sg;
+      sg.li = t.li;
+      sg.lj = t.lj;
+      sg.lk = t.lk;
+      sg.ll = t.ll;
+      sg.st = t.st;
+      sg.swap = t.swap;
+      sg.expcutoff = ecut;
+      sg.tile = ti;
+      sg.fp32 = t.fp32;
+      {
+        auto it = class_eps.find(std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32));
+        sg.prim_eps = it == class_eps.end() ? 0.0 : it->second;
+      }
+      sg.t0 = q;
+      sg.t1 = q + take;
+      sg.nout = nout;
+      sg.rec0 = cur.nrec;
+      sg.out_off = cur.out_size;
+      {
+        // flops of quartets [q, q + take): rows overlapping the range
+        double fl = 0;
+        const double fpp = flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll);
+        long long r = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
+        long long pos = q;
+        while (pos < q + take) {
+          const long long rend = std::min(t.row_prefix[r + 1], q + take);
+          const long long c0 = t.col0(r) + pos - t.row_prefix[r], c1 = t.col0(r) + rend - t.row_prefix[r];
+          fl += (double)o->pair_nprim[t.rows[r]] * (double)(t.cum_np[c1] - t.cum_np[c0]) * fpp;
+          pos = rend;
+          ++r;
+        }
+        sg.flops = fl + take * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
+      }
+      cur.pieces.push_back(sg);
+      cur.nrec += take;
+      cur.out_size += take * nout;
+      q += take;
+    }
+  }
+  if (!cur.pieces.empty()) {
+    p->chunks.push_back(cur);
+    max_recs = std::max(max_recs, cur.nrec);
+  }
+  // 4. device buffers
+  p->rec_capacity = max_recs;
+  bool ok = true;
+  if (max_recs > 0) ok = cudaMalloc(&p->d_recs, sizeof(QuartetRec) * max_recs) == cudaSuccess;
+  for (Tile& t : p->tiles) {
+    if (!ok) break;
+    ok = cudaMalloc(&t.d_rows, sizeof(int) * t.rows.size()) == cudaSuccess &&
+         cudaMalloc(&t.d_cols, sizeof(int) * t.cols.size()) == cudaSuccess &&
+         cudaMalloc(&t.d_prefix, sizeof(long long) * t.row_prefix.size()) == cudaSuccess;
+    if (ok && !t.colstart.empty()) {
+      ok = cudaMalloc(&t.d_colstart, sizeof(int) * t.colstart.size()) == cudaSuccess;
+      if (ok) cudaMemcpy(t.d_colstart, t.colstart.data(), sizeof(int) * t.colstart.size(), cudaMemcpyHostToDevice);
+    }
+    if (ok) {
+      cudaMemcpy(t.d_rows, t.rows.data(), sizeof(int) * t.rows.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(t.d_prefix, t.row_prefix.data(), sizeof(long long) * t.row_prefix.size(), cudaMemcpyHostToDevice);
+    }
+  }
+  // merge each chunk's tile pieces into one segment per kernel class (records of a class are
+  // contiguous; each record carries its chunk-relative output offset)
+  for (Chunk& ch : p->chunks) {
+    std::vector<int> order;
+    std::map<std::tuple<int, int, int, int, int, int>, int> first;
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < (int)ch.pieces.size(); ++i) {
+      const Segment& pc = ch.pieces[i];
+      auto key = std::make_tuple(pc.li, pc.lj, pc.lk, pc.ll, (int)pc.fp32, (int)pc.swap);
+      auto it = first.find(key);
+      if (it == first.end()) {
+        first[key] = (int)members.size();
+        members.push_back({i});
+      } else {
+        members[it->second].push_back(i);
+      }
+    }
+    ch.segs.clear();
+    long long rec = 0;
+    for (auto& mem : members) {
+      const Segment& p0 = ch.pieces[mem[0]];
+      Segment m;
+      m.li = p0.li;
+      m.lj = p0.lj;
+      m.lk = p0.lk;
+      m.ll = p0.ll;
+      m.st = p0.st;
+      m.expcutoff = p0.expcutoff;
+      m.tile = -2;
+      m.fp32 = p0.fp32;
+      m.prim_eps = p0.prim_eps;
+      m.swap = p0.swap;
+      m.rec0 = rec;
+      m.out_off = 0;
+      m.range0 = (int)p->ranges.size();
+      for (int i : mem) {
+        const Segment& pc = ch.pieces[i];
+        const Tile& t = p->tiles[pc.tile];
+        GenRange g;
+        g.rows = t.d_rows;
+        g.cols = t.d_cols;
+        g.prefix = t.d_prefix;
+        g.nrows = (int)t.rows.size();
+        g.swap = t.swap ? 1 : 0;
+        g.colstart = t.d_colstart;
+        g.t0 = pc.t0;
+        g.t1 = pc.t1;
+        g.rec_off = m.nrec;
+        g.out_off = pc.out_off;
+        g.nout = pc.nout;
+        p->ranges.push_back(g);
+        m.nrec += pc.t1 - pc.t0;
+        m.flops += pc.flops;
+      }
+      m.nranges = (int)p->ranges.size() - m.range0;
+      rec += m.nrec;
+      ch.segs.push_back(m);
+    }
+  }
+  if (ok && !p->ranges.empty()) {
+    ok = cudaMalloc(&p->d_ranges, sizeof(GenRange) * p->ranges.size()) == cudaSuccess;
+    if (ok) cudaMemcpy(p->d_ranges, p->ranges.data(), sizeof(GenRange) * p->ranges.size(), cudaMemcpyHostToDevice);
+  }
+  if (!ok) {
+    free_plan_device(p);
+    delete p;
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the screened plan failed");
+    return CINTX_STATUS_ALLOCATION_FAILED;
+  }
+  long long maxc = 0;
+  for (const Chunk& c : p->chunks) maxc = std::max(maxc, c.out_size);
+  p->stats.nquartets = nq_total;
+  p->stats.nintegrals = nint_total;
+  p->stats.nchunks = (int64_t)p->chunks.size();
+  p->stats.max_chunk_doubles = maxc;
+  p->stats.nprim_quartets = nprimq;
+  p->stats.flops = flops;
+  p->stats.nquartets_fp32 = nq_fp32;
+  {
+    long long db = (long long)sizeof(QuartetRec) * max_recs;
+    for (const Tile& t : p->tiles)
+      db += (long long)(sizeof(int) * (t.rows.size() + t.cols.size()) + sizeof(long long) * t.row_prefix.size());
+    p->stats.device_bytes = db;
+  }
+  *plan = p;
+  return CINTX_STATUS_SUCCESS;
+}
+
 static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk,
                           double fp32_budget, double prim_budget) {
   clear_error();
@@ -1027,6 +1253,10 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
   if (B.nvirt != B.nbas) {
     set_error(CINTX_STATUS_UNSUPPORTED_API, "screened plans need single-contraction shells (nctr = 1)");
     return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (o->npv != B.nvirt) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "the int2e sweep needs an optimizer holding the pairs of every shell");
+    return CINTX_STATUS_INVALID_INPUT;
   }
   if (B.env[PTR_RANGE_OMEGA] != 0.0) {
     set_error(CINTX_STATUS_UNSUPPORTED_API, "range-separated Coulomb is not supported");
@@ -1086,8 +1316,7 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
   p->family = CINTX_INT2E;
   p->sph = sph != 0;
   const double ecut = expcutoff_2e(B.env.data());
-  long long nq_total = 0, nint_total = 0, nprimq = 0, nq_fp32 = 0;
-  double flops = 0;
+  long long nq_total = 0, nint_total = 0, nq_fp32 = 0;
   const int nt = (int)tlist.size();
   // tiles A >= B in type order (types are ordered by (la, lb, ...), so classes are valid)
   for (int A = 0; A < nt; ++A) {
@@ -1099,6 +1328,7 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
       t.lj = std::get<1>(tkeys[A]);
       t.lk = std::get<0>(tkeys[Bt]);
       t.ll = std::get<1>(tkeys[Bt]);
+      t.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
       const std::vector<int>& rows = tlist[A];
       const std::vector<int>& cols = tlist[Bt];
       std::vector<double> qcols(cols.size());
@@ -1164,210 +1394,138 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
       }
     }
   }
-  // flops: per tile class
-  {
-    // recompute nprim-weighted flops per tile
-    nprimq = 0;
-    for (const Tile& t : p->tiles) {
-      std::vector<long long> cum(t.cols.size() + 1, 0);
-      for (size_t c = 0; c < t.cols.size(); ++c) cum[c + 1] = cum[c] + o->pair_nprim[t.cols[c]];
-      long long tp = 0;
-      for (size_t r = 0; r < t.rows.size(); ++r) {
-        const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
-        tp += (long long)o->pair_nprim[t.rows[r]] * (cum[t.col0(r) + cnt] - cum[t.col0(r)]);
-      }
-      nprimq += tp;
-      const long long nq = t.row_prefix.back();
-      flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
-    }
+  return finish_screened(p, o, ecut, max_chunk, prim_budget, nq_total, nint_total, nq_fp32, plan);
+}
+
+// Diagonal Schwarz factors sqrt(max |block|) of a list of tuples of one family (spherical).
+static int diag_factors(CINTOpt* optp, int family, const std::vector<int>& tuples, int64_t n, std::vector<double>& q) {
+  std::vector<int64_t> off(std::max<int64_t>(n, 1));
+  CintxPlan* dp = nullptr;
+  int rc = cintx_plan_shells(&dp, optp, family, tuples.data(), n, 1, off.data());
+  if (rc) return rc;
+  const long long tot = dp->stats.nintegrals;
+  std::vector<double> out(std::max<long long>(tot, 1));
+  rc = cintx_plan_execute_host(dp, 0, out.data());
+  cintx_plan_destroy(dp);
+  if (rc) return rc;
+  q.assign(n, 0.0);
+  for (int64_t t = 0; t < n; ++t) {
+    const long long e1 = t + 1 < n ? off[t + 1] : tot;
+    double m = 0;
+    for (long long e = off[t]; e < e1; ++e) m = std::max(m, fabs(out[e]));
+    q[t] = sqrt(m);
   }
-  // primitive screening threshold per kernel class and precision: the dropped primitive
-  // quartets of one contracted quartet sum to at most prim_budget in its spherical block
-  std::map<std::tuple<int, int, int, int, int>, double> class_eps;
-  if (prim_budget > 0) {
-    std::map<std::tuple<int, int, int, int, int>, double> maxprod;
-    for (const Tile& t : p->tiles) {
-      int mr = 1, mc = 1;
-      for (int id : t.rows) mr = std::max(mr, o->pair_nprim[id]);
-      for (int id : t.cols) mc = std::max(mc, o->pair_nprim[id]);
-      auto key = std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32);
-      maxprod[key] = std::max(maxprod[key], (double)mr * mc);
-    }
-    for (auto& kv : maxprod) {
-      const int li = std::get<0>(kv.first), lj = std::get<1>(kv.first), lk = std::get<2>(kv.first),
-                ll = std::get<3>(kv.first);
-      const double amp = c2s_amp(li, p->sph) * c2s_amp(lj, p->sph) * c2s_amp(lk, p->sph) * c2s_amp(ll, p->sph);
-      class_eps[kv.first] = prim_budget / (kv.second * amp);
-    }
-  }
-  // 3. chunks: greedy fill up to max_chunk doubles, splitting tiles at quartet boundaries
-  Chunk cur;
-  long long max_recs = 0;
-  for (int ti = 0; ti < (int)p->tiles.size(); ++ti) {
-    const Tile& t = p->tiles[ti];
-    const long long nq = t.row_prefix.back();
-    const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
-                           nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
-    long long q = 0;
-    while (q < nq) {
-      long long room = (max_chunk - cur.out_size) / nout;
-      if (room <= 0) {
-        if (cur.pieces.empty()) room = 1;  // a single block larger than the chunk limit
-        else {
-          p->chunks.push_back(cur);
-          max_recs = std::max(max_recs, cur.nrec);
-          cur = Chunk();
-          continue;
-        }
-      }
-      const long long take = std::min(room, nq - q);
-      Segment sg;
-      sg.li = t.li;
-      sg.lj = t.lj;
-      sg.lk = t.lk;
-      sg.ll = t.ll;
-      sg.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
-      sg.expcutoff = ecut;
-      sg.tile = ti;
-      sg.fp32 = t.fp32;
-      {
-        auto it = class_eps.find(std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32));
-        sg.prim_eps = it == class_eps.end() ? 0.0 : it->second;
-      }
-      sg.t0 = q;
-      sg.t1 = q + take;
-      sg.nout = nout;
-      sg.rec0 = cur.nrec;
-      sg.out_off = cur.out_size;
-      {
-        // flops of quartets [q, q + take): rows overlapping the range
-        double fl = 0;
-        const double fpp = flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll);
-        long long r = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
-        long long pos = q;
-        while (pos < q + take) {
-          const long long rend = std::min(t.row_prefix[r + 1], q + take);
-          const long long c0 = t.col0(r) + pos - t.row_prefix[r], c1 = t.col0(r) + rend - t.row_prefix[r];
-          fl += (double)o->pair_nprim[t.rows[r]] * (double)(t.cum_np[c1] - t.cum_np[c0]) * fpp;
-          pos = rend;
-          ++r;
-        }
-        sg.flops = fl + take * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
-      }
-      cur.pieces.push_back(sg);
-      cur.nrec += take;
-      cur.out_size += take * nout;
-      q += take;
-    }
-  }
-  if (!cur.pieces.empty()) {
-    p->chunks.push_back(cur);
-    max_recs = std::max(max_recs, cur.nrec);
-  }
-  // 4. device buffers
-  p->rec_capacity = max_recs;
-  bool ok = true;
-  if (max_recs > 0) ok = cudaMalloc(&p->d_recs, sizeof(QuartetRec) * max_recs) == cudaSuccess;
-  for (Tile& t : p->tiles) {
-    if (!ok) break;
-    ok = cudaMalloc(&t.d_rows, sizeof(int) * t.rows.size()) == cudaSuccess &&
-         cudaMalloc(&t.d_cols, sizeof(int) * t.cols.size()) == cudaSuccess &&
-         cudaMalloc(&t.d_prefix, sizeof(long long) * t.row_prefix.size()) == cudaSuccess;
-    if (ok && !t.colstart.empty()) {
-      ok = cudaMalloc(&t.d_colstart, sizeof(int) * t.colstart.size()) == cudaSuccess;
-      if (ok) cudaMemcpy(t.d_colstart, t.colstart.data(), sizeof(int) * t.colstart.size(), cudaMemcpyHostToDevice);
-    }
-    if (ok) {
-      cudaMemcpy(t.d_rows, t.rows.data(), sizeof(int) * t.rows.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(t.d_prefix, t.row_prefix.data(), sizeof(long long) * t.row_prefix.size(), cudaMemcpyHostToDevice);
-    }
-  }
-  // merge each chunk's tile pieces into one segment per kernel class (records of a class are
-  // contiguous; each record carries its chunk-relative output offset)
-  for (Chunk& ch : p->chunks) {
-    std::vector<int> order;
-    std::map<std::tuple<int, int, int, int, int>, int> first;
-    std::vector<std::vector<int>> members;
-    for (int i = 0; i < (int)ch.pieces.size(); ++i) {
-      const Segment& pc = ch.pieces[i];
-      auto key = std::make_tuple(pc.li, pc.lj, pc.lk, pc.ll, (int)pc.fp32);
-      auto it = first.find(key);
-      if (it == first.end()) {
-        first[key] = (int)members.size();
-        members.push_back({i});
-      } else {
-        members[it->second].push_back(i);
-      }
-    }
-    ch.segs.clear();
-    long long rec = 0;
-    for (auto& mem : members) {
-      const Segment& p0 = ch.pieces[mem[0]];
-      Segment m;
-      m.li = p0.li;
-      m.lj = p0.lj;
-      m.lk = p0.lk;
-      m.ll = p0.ll;
-      m.st = p0.st;
-      m.expcutoff = p0.expcutoff;
-      m.tile = -2;
-      m.fp32 = p0.fp32;
-      m.prim_eps = p0.prim_eps;
-      m.rec0 = rec;
-      m.out_off = 0;
-      m.range0 = (int)p->ranges.size();
-      for (int i : mem) {
-        const Segment& pc = ch.pieces[i];
-        const Tile& t = p->tiles[pc.tile];
-        GenRange g;
-        g.rows = t.d_rows;
-        g.cols = t.d_cols;
-        g.prefix = t.d_prefix;
-        g.nrows = (int)t.rows.size();
-        g.pad = 0;
-        g.colstart = t.d_colstart;
-        g.t0 = pc.t0;
-        g.t1 = pc.t1;
-        g.rec_off = m.nrec;
-        g.out_off = pc.out_off;
-        g.nout = pc.nout;
-        p->ranges.push_back(g);
-        m.nrec += pc.t1 - pc.t0;
-        m.flops += pc.flops;
-      }
-      m.nranges = (int)p->ranges.size() - m.range0;
-      rec += m.nrec;
-      ch.segs.push_back(m);
-    }
-  }
-  if (ok && !p->ranges.empty()) {
-    ok = cudaMalloc(&p->d_ranges, sizeof(GenRange) * p->ranges.size()) == cudaSuccess;
-    if (ok) cudaMemcpy(p->d_ranges, p->ranges.data(), sizeof(GenRange) * p->ranges.size(), cudaMemcpyHostToDevice);
-  }
-  if (!ok) {
-    free_plan_device(p);
-    delete p;
-    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the screened plan failed");
-    return CINTX_STATUS_ALLOCATION_FAILED;
-  }
-  long long maxc = 0;
-  for (const Chunk& c : p->chunks) maxc = std::max(maxc, c.out_size);
-  p->stats.nquartets = nq_total;
-  p->stats.nintegrals = nint_total;
-  p->stats.nchunks = (int64_t)p->chunks.size();
-  p->stats.max_chunk_doubles = maxc;
-  p->stats.nprim_quartets = nprimq;
-  p->stats.flops = flops;
-  p->stats.nquartets_fp32 = nq_fp32;
-  {
-    long long db = (long long)sizeof(QuartetRec) * max_recs;
-    for (const Tile& t : p->tiles)
-      db += (long long)(sizeof(int) * (t.rows.size() + t.cols.size()) + sizeof(long long) * t.row_prefix.size());
-    p->stats.device_bytes = db;
-  }
-  *plan = p;
   return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sph, int64_t max_chunk,
+                                int norb) {
+  clear_error();
+  if (!plan) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  *plan = nullptr;
+  Opt* o = as_opt(optp);
+  if (!o) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "opt is not a handle created by this library");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  const Basis& B = o->basis;
+  const int nb = B.nbas;
+  if (B.nvirt != B.nbas) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "screened plans need single-contraction shells (nctr = 1)");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (norb < 1 || norb >= nb || o->npv < norb) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "norb must split the basis into orbital shells [0, norb) whose pairs the "
+                                          "optimizer holds and auxiliary shells [norb, nbas)");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  if (B.env[PTR_RANGE_OMEGA] != 0.0) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "range-separated Coulomb is not supported");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (max_chunk <= 0) max_chunk = 1LL << 28;
+  const int npo = norb * (norb + 1) / 2;  // pair ids of the orbital pairs (u < norb)
+  const int naux = nb - norb;
+  // 1. Schwarz factors: (ab|ab) for orbital pairs, (k|k) for auxiliary shells
+  std::vector<int> dt((size_t)npo * 4), kt((size_t)naux * 2);
+  for (int id = 0; id < npo; ++id) {
+    dt[4 * id] = dt[4 * id + 2] = o->pair_a[id];
+    dt[4 * id + 1] = dt[4 * id + 3] = o->pair_b[id];
+  }
+  for (int k = 0; k < naux; ++k) kt[2 * k] = kt[2 * k + 1] = norb + k;
+  std::vector<double> Q, Qk;
+  int rc = diag_factors(optp, CINTX_INT2E, dt, npo, Q);
+  if (!rc) rc = diag_factors(optp, CINTX_INT2C2E, kt, naux, Qk);
+  if (rc) return rc;
+  double qmax = 0, qkmax = 0;
+  for (double v : Q) qmax = std::max(qmax, v);
+  for (double v : Qk) qkmax = std::max(qkmax, v);
+  // 2. row types (la, lb, nprim_a, nprim_b) of orbital pairs and column types (lk, nprim_k) of
+  // auxiliary unit pairs, each sorted by decreasing Schwarz factor
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> rtypes;
+  std::map<std::pair<int, int>, std::vector<int>> ctypes;
+  std::vector<double> qpair(o->npairs + B.nvirt, 0.0);
+  for (int id = 0; id < npo; ++id) {
+    qpair[id] = Q[id];
+    if (!(Q[id] * qkmax >= cutoff) || o->pair_nprim[id] == 0) continue;
+    rtypes[std::make_tuple(o->pair_la[id], o->pair_lb[id], B.sh[o->pair_a[id]].nprim, B.sh[o->pair_b[id]].nprim)]
+        .push_back(id);
+  }
+  for (int k = 0; k < naux; ++k) {
+    const int id = o->npairs + norb + k;
+    qpair[id] = Qk[k];
+    if (!(Qk[k] * qmax >= cutoff) || o->pair_nprim[id] == 0) continue;
+    ctypes[std::make_pair(B.sh[norb + k].l, B.sh[norb + k].nprim)].push_back(id);
+  }
+  auto by_q = [&](int x, int y) { return qpair[x] > qpair[y]; };
+  CintxPlan* p = new CintxPlan();
+  p->opt = o;
+  p->family = CINTX_INT3C2E;
+  p->sph = sph != 0;
+  long long nq_total = 0, nint_total = 0;
+  for (auto& rk : rtypes) {
+    std::vector<int> rows = rk.second;
+    std::stable_sort(rows.begin(), rows.end(), by_q);
+    const int la = std::get<0>(rk.first), lb = std::get<1>(rk.first);
+    for (auto& ck : ctypes) {
+      std::vector<int> cols = ck.second;
+      std::stable_sort(cols.begin(), cols.end(), by_q);
+      const int lk = ck.first.first;
+      const long long ni = nsph_or_cart(la, p->sph), nj = nsph_or_cart(lb, p->sph), nk = nsph_or_cart(lk, p->sph);
+      Tile t;
+      t.typeA = t.typeB = 0;
+      // block layout out[i + ni*(j + nj*k)] for the tuple (a, b, k); the kernel's first pair is
+      // the larger in (l, l') order, so an auxiliary shell of higher l than a swaps the pairs
+      t.swap = lk > la;
+      if (!t.swap) {
+        t.li = la; t.lj = lb; t.lk = lk; t.ll = 0;
+        t.st.s0 = 1; t.st.s1 = ni; t.st.s2 = ni * nj; t.st.s3 = 0;
+      } else {
+        t.li = lk; t.lj = 0; t.lk = la; t.ll = lb;
+        t.st.s0 = ni * nj; t.st.s1 = 0; t.st.s2 = 1; t.st.s3 = ni;
+      }
+      t.row_prefix.push_back(0);
+      for (int r : rows) {
+        const double qa = qpair[r];
+        const long long cnt = std::partition_point(cols.begin(), cols.end(),
+                                                   [&](int c) { return qa * qpair[c] >= cutoff; }) - cols.begin();
+        if (cnt <= 0) continue;
+        t.rows.push_back(r);
+        t.row_prefix.push_back(t.row_prefix.back() + cnt);
+      }
+      if (t.rows.empty()) continue;
+      t.cols = cols;
+      t.cum_np.assign(cols.size() + 1, 0);
+      for (size_t c = 0; c < cols.size(); ++c) t.cum_np[c + 1] = t.cum_np[c] + o->pair_nprim[cols[c]];
+      nq_total += t.row_prefix.back();
+      nint_total += t.row_prefix.back() * ni * nj * nk;
+      p->tiles.push_back(t);
+    }
+  }
+  return finish_screened(p, o, expcutoff_3c(B.env.data()), max_chunk, 0.0, nq_total, nint_total, 0, plan);
 }
 
 int64_t cintx_opt_device_bytes(CINTOpt* optp) {

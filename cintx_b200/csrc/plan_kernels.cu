@@ -64,8 +64,9 @@ __global__ void gen_range_quartets(const GenRange* __restrict__ ranges, int nran
       else b = mid - 1;
     }
     QuartetRec q;
-    q.pij = g.rows[a];
-    q.pkl = g.cols[(g.colstart ? g.colstart[a] : 0) + (t - g.prefix[a])];
+    const int row = g.rows[a], col = g.cols[(g.colstart ? g.colstart[a] : 0) + (t - g.prefix[a])];
+    q.pij = g.swap ? col : row;
+    q.pkl = g.swap ? row : col;
     q.out = g.out_off + (r - g.rec_off) * g.nout;
     recs[r] = q;
   }

@@ -143,6 +143,23 @@ CINTX_API int cintx_plan_int2e_screened_mixed(CintxPlan **plan, CINTOpt *opt, do
                                               int64_t max_chunk_doubles, double fp32_budget,
                                               double prim_budget);
 
+/* Optimizer for density-fitting sweeps over a basis whose first npair_shells shells are the
+ * orbital shells and the rest auxiliary shells: shell pairs are built only among the orbital
+ * shells (the (ij| side of int3c2e), unit pairs for every shell (the |k) side and int2c2e).  The
+ * handle works with every entry point; tuples needing a pair it does not hold are rejected.  No
+ * counterpart in libcint (CINTall_3c2e_optimizer, optimizer.c:193, builds every pair).  Returns a
+ * status code; *opt is NULL on failure. */
+CINTX_API int cintx_optimizer_pair_shells(CINTOpt **opt, const int *atm, int natm, const int *bas, int nbas,
+                                          const double *env, int npair_shells);
+
+/* Density-fitting 3-centre sweep: every (ab|k) with a >= b orbital shells in [0, norb) and k an
+ * auxiliary shell in [norb, nbas) whose Schwarz bound sqrt(max|(ab|ab)|) sqrt(max|(k|k)|) reaches
+ * cutoff, as int3c2e_sph/int3c2e_cart blocks (libcint cint3c2e.c:693) out[i + ni*(j + nj*k)] for
+ * the tuple (a, b, k) with a the shell of higher l (equal l: higher index), chunked like
+ * cintx_plan_int2e_screened; cintx_plan_chunk_quartets reports tuples (a, b, k, -1). */
+CINTX_API int cintx_plan_int3c2e_screened(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
+                                          int64_t max_chunk_doubles, int norb);
+
 /* Plan statistics. */
 typedef struct {
   int64_t nquartets;        /* shell tuples in the plan */
