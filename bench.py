@@ -46,6 +46,17 @@ WORKLOADS = {
                               "Schwarz 1e-12"),
     "water3": (M.water_like, "3-atom water-like molecule (O + 2 H), all quartets above 1e-12"),
 }
+# density-fitting workloads: the orbital molecule plus a per-atom auxiliary basis
+# (6s 5p 4d 3f 2g single primitives, exponents log-uniform in [0.05, 5e3])
+DF_WORKLOADS = {
+    "mol120_df": (M.mol120, "mol120_spdf plus the per-atom auxiliary basis (9600 aux functions): int3c2e_sph over "
+                            "orbital pairs x aux shells with Schwarz bound >= 1e-12, plus the int2c2e_sph metric "
+                            "over aux shell pairs k >= l"),
+    "mol40_df": (M.mol40, "mol40_spd plus the per-atom auxiliary basis (3200 aux functions): int3c2e_sph over "
+                          "orbital pairs x aux shells with Schwarz bound >= 1e-12, plus int2c2e_sph over aux "
+                          "pairs k >= l"),
+}
+
 SCHWARZ = 1e-12
 # tuned form: quartets whose estimated FP32 error is below this use FP32 recurrences; off by default
 # (5e-11 selects 0.5% of the mol40 quartets and measures 4.6% slower: the FP64 pipe is not the bound)
@@ -60,7 +71,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="mol40_spd", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mol40_spd", choices=sorted(WORKLOADS) + sorted(DF_WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk-doubles", type=int, default=1 << 28)
     ap.add_argument("--branches", type=int, default=4)
@@ -267,6 +278,90 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+def df_problem(name):
+    fn, desc = DF_WORKLOADS[name]
+    base = fn()
+    mol = M.with_aux(base)
+    norb = base.nbas
+    naux = mol.nbas - norb
+    kk, ll = np.tril_indices(naux)
+    aux_pairs = np.stack([norb + kk, norb + ll], axis=1).astype(np.int32)
+    return mol, norb, aux_pairs, desc
+
+
+class DFTriples:
+    """The density-fitting sweep's tuple set ((ab|k), a >= b orbital, k auxiliary, Schwarz bound
+    >= cutoff) built on the host from libcint Schwarz factors, with uniform sampling."""
+
+    def __init__(self, mol, norb, cutoff):
+        from concurrent.futures import ThreadPoolExecutor
+        from oracle import RefLibcint
+        ref = RefLibcint()
+        pairs = [(i, j) for i in range(norb) for j in range(i + 1)]
+        aux = list(range(norb, mol.nbas))
+        with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+            q = np.array(list(ex.map(lambda p: np.sqrt(np.abs(ref.int2e((p[0], p[1], p[0], p[1]), mol)[0]).max()),
+                                     pairs, chunksize=256)))
+            qk = np.array(list(ex.map(lambda k: np.sqrt(np.abs(ref.int2c2e((k, k), mol)[0]).max()), aux)))
+        order = np.argsort(-qk, kind="stable")
+        self.aux, self.qk = np.array(aux)[order], qk[order]
+        self.pairs = np.array(pairs, dtype=np.int32)
+        self.count = np.searchsorted(-self.qk, -(cutoff / np.maximum(q, 1e-300)), side="right")
+        l = mol.bas[:, 1]
+        ns = (2 * l[self.pairs[:, 0]] + 1) * (2 * l[self.pairs[:, 1]] + 1)
+        cum = np.concatenate([[0], np.cumsum(2 * l[self.aux] + 1)])
+        self.nquartets = int(self.count.sum())
+        self.nintegrals = int((ns * cum[self.count]).sum())
+        self.prob = self.count / self.count.sum()
+
+    def sample(self, n, seed):
+        rng = np.random.default_rng(seed)
+        i = rng.choice(len(self.pairs), size=n, p=self.prob)
+        k = self.aux[(rng.random(n) * self.count[i]).astype(np.int64)]
+        return np.stack([self.pairs[i, 0], self.pairs[i, 1], k, np.full(n, -1)], axis=1).astype(np.int32)
+
+
+def df_reference_arm(args):
+    """libcint int3c2e_sph + int2c2e_sph on the host cores over the DF sweep's tuple set."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if not os.path.exists(REF_DRIVER):
+        print(json.dumps({"impl": "reference", "unavailable": "libcint was not built from the reference "
+                          "sources (oracle/_ref missing)"}))
+        return
+    mol, norb, aux_pairs, desc = df_problem(args.workload)
+    tri = DFTriples(mol, norb, SCHWARZ)
+    threads = os.cpu_count() or 1
+    l = mol.bas[:, 1]
+    n2int = int(((2 * l[aux_pairs[:, 0]] + 1) * (2 * l[aux_pairs[:, 1]] + 1)).sum())
+    two = np.stack([aux_pairs[:, 0], np.full(len(aux_pairs), -1), aux_pairs[:, 1], np.full(len(aux_pairs), -1)],
+                   axis=1).astype(np.int32)
+    cal = run_libcint(mol, tri.sample(2000, 100), threads)
+    per_q = cal["seconds"] / 2000
+    nsamp = int(min(2_000_000, max(2000, 8.0 / max(per_q, 1e-9))))
+    rng = np.random.default_rng(7)
+    times = []
+    for s_ in range(args.warmup + args.steps):
+        r3 = run_libcint(mol, tri.sample(nsamp, 1000 + s_), threads)
+        r2 = run_libcint(mol, two[rng.choice(len(two), size=min(len(two), 20000), replace=False)], threads)
+        if s_ >= args.warmup:
+            times.append(r3["seconds"] / nsamp * tri.nquartets + r2["seconds"] / min(len(two), 20000) * len(two))
+    t = statistics.mean(times)
+    value = (tri.nintegrals + n2int) / t / 1e9
+    line = {"metric": "int3c2e_sph + int2c2e_sph Gint/s, density fitting (libcint CPU reference)", "value": value,
+            "unit": "Gint/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": args.workload, "description": desc, "ntriples": tri.nquartets,
+                       "nintegrals": tri.nintegrals + n2int, "schwarz_cutoff": SCHWARZ},
+            "cpu_baseline": {"value": value, "unit": "Gint/s", "cores": threads, "kind": "reference",
+                             "sample": "%d seeded uniform (ab|k) triples and 20000 (k|l) pairs per step, "
+                                       "extrapolated by count" % nsamp},
+            "e2e": {"value": value, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------ our arm
 def fp64_peak(cx, torch):
     """FP64 FMA pipe throughput of this GPU (TFLOP/s), best of 3."""
@@ -290,33 +385,45 @@ def fp64_peak(cx, torch):
 def timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=False):
     """Warm-up, then exactly args.steps timed passes of `plan` over the rank's chunks (one CUDA
     graph per pass unless --no-graph), L2 flushed between passes outside the events.  With
-    tune, the plan's launch shapes are autotuned first on the rank's heaviest chunk."""
+    tune, the plan's launch shapes are autotuned first (each class on its largest segment)."""
+    return timed_multi(cx, torch, [(plan, mine)], args, stream, local, world, tune)
+
+
+def timed_multi(cx, torch, items, args, stream, local, world, tune=False):
+    """As timed_sweep for several plans run back to back in one step: items = [(plan, chunks)]."""
     import torch.distributed as dist
-    st = plan.stats
-    ring = torch.empty(max(st.max_chunk_doubles, 1), dtype=torch.float64, device="cuda")
+    rings = [torch.empty(max(p.stats.max_chunk_doubles, 1), dtype=torch.float64, device="cuda") for p, _ in items]
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     tuning = None
-    if tune and mine:
+    if tune:
         t0 = time.perf_counter()
-        plan.autotune(ring.data_ptr(), chunk=-1, stream=stream.cuda_stream, reps=2)
         lanes = {}
-        for c in mine:
-            for cl, n in zip(plan.segments(c)[0], plan.segment_lanes(c)):
-                lanes["(%d%d|%d%d)" % tuple(cl)] = int(n)
+        for (plan, mine), ring in zip(items, rings):
+            if not mine:
+                continue
+            plan.autotune(ring.data_ptr(), chunk=-1, stream=stream.cuda_stream, reps=2)
+            for c in mine:
+                for cl, n in zip(plan.segments(c)[0], plan.segment_lanes(c)):
+                    lanes["(%d%d|%d%d)" % tuple(cl)] = int(n)
         tuning = {"seconds": time.perf_counter() - t0, "lanes_per_quartet": dict(sorted(lanes.items()))}
     use_graph = not args.no_graph
     if use_graph:
         try:
-            plan.graph_build(ring.data_ptr(), chunks=mine, nbranch=args.branches)
+            for (plan, mine), ring in zip(items, rings):
+                if mine:
+                    plan.graph_build(ring.data_ptr(), chunks=mine, nbranch=args.branches)
         except cx.CintxError:
             use_graph = False
 
     def step():
-        if use_graph:
-            plan.graph_launch(stream.cuda_stream)
-        else:
-            for c in mine:
-                plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
+        for (plan, mine), ring in zip(items, rings):
+            if not mine:
+                continue
+            if use_graph:
+                plan.graph_launch(stream.cuda_stream)
+            else:
+                for c in mine:
+                    plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -344,8 +451,8 @@ def timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=False):
     launches = cx.launch_count() - launches0
     clk = clocks.stop()
     ms = max_over_ranks(sum(step_ms), device="cuda") / args.steps
-    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": ring,
-            "tuning": tuning}
+    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": rings[0],
+            "rings": rings, "tuning": tuning}
 
 
 def class_profile(torch, plan, mine, ring, stream):
@@ -567,12 +674,148 @@ def our_arm(args):
     opt.close()
 
 
+def df_arm(args):
+    """Density-fitting sweep on the GPU: int3c2e_sph (screened (ab|k) plan, chunks sharded over
+    ranks by flops) plus the int2c2e_sph metric (rank 0), one CUDA graph each per step."""
+    import torch
+    import torch.distributed as dist
+
+    import cintx_b200 as cx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    mol, norb, aux_pairs, desc = df_problem(args.workload)
+    tuned = args.form == "tuned"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def make(o):
+        p3 = cx.Plan.screened_3c(o, norb, SCHWARZ, max_chunk_doubles=args.chunk_doubles)
+        p2 = cx.Plan.shells(o, cx.INT2C2E, aux_pairs)
+        return p3, p2
+
+    opt = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
+    p3, p2 = make(opt)
+    s3, s2 = p3.stats, p2.stats
+    mine3 = chunks_of(assign_chunks([float(p3.segments(c)[2].sum()) for c in range(s3.nchunks)], world), rank)
+    mine2 = [0] if rank == 0 else []
+    run = timed_multi(cx, torch, [(p3, mine3), (p2, mine2)], args, stream, local, world,
+                      tune=tuned and not args.no_autotune)
+    nint = s3.nintegrals + s2.nintegrals
+    value = nint / (run["ms"] * 1e-3) / 1e9
+    plain = err = None
+    if tuned:
+        q3, q2 = make(opt)  # default launch shapes
+        prun = timed_multi(cx, torch, [(q3, mine3), (q2, mine2)], args, stream, local, world, tune=False)
+        plain = {"value": nint / (prun["ms"] * 1e-3) / 1e9, "ms_per_step": prun["ms"]}
+        if rank == 0 and mine3:
+            c = mine3[0]
+            a, b = run["rings"][0], prun["rings"][0]
+            p3.execute(a.data_ptr(), chunk=c, stream=stream.cuda_stream)
+            q3.execute(b.data_ptr(), chunk=c, stream=stream.cuda_stream)
+            stream.synchronize()
+            n = p3.chunk_size(c)
+            err = {"max_abs": float((a[:n] - b[:n]).abs().max()), "integrals_checked": n,
+                   "reference": "the same chunk with the default launch shapes"}
+        q3.close()
+        q2.close()
+    per_class = class_profile(torch, p3, mine3, run["rings"][0], stream)
+    peak64 = fp64_peak(cx, torch)
+    roof = None
+    if per_class:
+        top = max(per_class.items(), key=lambda kv: kv[1]["ms"])
+        d = top[1]
+        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
+        roof = {"bound": "fp64", "kernel": "eri4c_kernel" + top[0], "achieved": achieved, "peak": peak64,
+                "unit": "TFLOP/s", "frac": achieved / peak64,
+                "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "share_of_step": d["ms"] / sum(v["ms"] for v in per_class.values()), "traffic": None}
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    line = {"metric": "int3c2e_sph + int2c2e_sph Gint/s, density fitting (%s form)" % ("tuned" if tuned else "plain"),
+            "value": value, "unit": "Gint/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": run["ms"], "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded molecule and auxiliary basis; no dataset)",
+            "config": {"workload": args.workload, "description": desc, "ntriples": s3.nquartets,
+                       "nintegrals_3c": s3.nintegrals, "nintegrals_2c": s2.nintegrals, "nchunks": s3.nchunks,
+                       "norb_shells": norb, "naux_shells": mol.nbas - norb, "schwarz_cutoff": SCHWARZ,
+                       "model_flops_per_step": s3.flops + s2.flops,
+                       "form": "autotuned launch shapes, graph-batched" if tuned and not args.no_autotune
+                               else "default launch shapes, graph-batched",
+                       "l2": "flushed between steps (512 MiB write outside the step events)"},
+            "quartets_per_s": (s3.nquartets + s2.nquartets) / (run["ms"] * 1e-3),
+            "gpu_launches": run["launches"], "clocks": run["clocks"], "roofline": roof,
+            "per_class": {k: {"ms": round(v["ms"], 4), "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3),
+                              "quartets": v["quartets"]}
+                          for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:12]}}
+    if run["tuning"] is not None:
+        line["autotune"] = run["tuning"]
+    if plain is not None:
+        line["plain_fp64"] = plain
+        line["tuned_over_plain"] = value / plain["value"]
+    if err is not None:
+        line["error_vs_default_shapes"] = err
+    if not args.no_e2e:
+        # end to end from host arrays: optimizer, both plans, evaluation and D2H of every chunk into
+        # a page-locked host buffer (one chunk at a time: the 3-centre output exceeds host memory)
+        host = torch.empty(max(s3.max_chunk_doubles, s2.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
+        times = []
+        for s_ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
+            e3, e2 = make(o2)
+            if tuned and not args.no_autotune:
+                e3.use_tuned_shapes()
+                e2.use_tuned_shapes()
+            for c in range(e3.stats.nchunks):
+                e3.execute_host(host, chunk=c)
+            e2.execute_host(host)
+            times.append(time.perf_counter() - t0)
+            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + e3.stats.device_bytes
+            e3.close()
+            e2.close()
+            o2.close()
+        te = times[-1]
+        line["e2e"] = {"value": nint / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(nint * 8), "seconds_per_step": te,
+                       "includes": "optimizer from host atm/bas/env, both plans (Schwarz passes), evaluation and "
+                                   "D2H of every integral, chunk by chunk"}
+    if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
+        n3 = min(200000, s3.nquartets)
+        r3 = run_libcint(mol, p3.sample_quartets(n3, 1), os.cpu_count() or 1)
+        n2 = min(20000, s2.nquartets)
+        r2 = run_libcint(mol, p2.sample_quartets(n2, 2), os.cpu_count() or 1)
+        t_full = r3["seconds"] / n3 * s3.nquartets + r2["seconds"] / n2 * s2.nquartets
+        line["cpu_baseline"] = {"value": nint / t_full / 1e9, "unit": "Gint/s", "cores": int(r3["threads"]),
+                                "kind": "reference",
+                                "sample": "%d (ab|k) triples and %d (k|l) pairs drawn uniformly from the plans, "
+                                          "libcint int3c2e_sph/int2c2e_sph with optimizers, OpenMP dynamic; "
+                                          "extrapolated by count" % (n3, n2)}
+    print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    p3.close()
+    p2.close()
+    opt.close()
+
+
 def main():
     args = parse()
+    df = args.workload in DF_WORKLOADS
     if args.impl == "reference":
-        reference_arm(args)
+        (df_reference_arm if df else reference_arm)(args)
     else:
-        our_arm(args)
+        (df_arm if df else our_arm)(args)
 
 
 if __name__ == "__main__":
