@@ -76,6 +76,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute.restype = _i
     L.cintx_plan_execute_host.argtypes = [_vp, _i64, _dp]
     L.cintx_plan_execute_host.restype = _i
+    L.cintx_plan_execute_host_ring.argtypes = [_vp, _dp, _i64, ctypes.c_void_p, ctypes.c_void_p]
+    L.cintx_plan_execute_host_ring.restype = _i
     L.cintx_plan_autotune.argtypes = [_vp, _i64, ctypes.c_void_p, ctypes.c_void_p, _i]
     L.cintx_plan_autotune.restype = _i
     L.cintx_plan_use_tuned_shapes.argtypes = [_vp]
@@ -367,6 +369,22 @@ class Plan:
             raise ValueError("out holds %d doubles, the output needs %d" % (out.size, need))
         _check(lib.cintx_plan_execute_host(self.handle, chunk, out.ctypes.data_as(_dp)))
         return out
+
+    _CHUNK_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, _dp, ctypes.c_int64)
+
+    def execute_host_ring(self, ring: np.ndarray, on_chunk=None):
+        """Evaluate every chunk through a two-slot host ring (ring.size >= 2 x max chunk);
+        on_chunk(chunk, array_view) is called for each chunk in order before its slot is reused."""
+        if ring.dtype != np.float64 or not ring.flags.c_contiguous:
+            raise ValueError("ring must be a C-contiguous float64 array")
+        cb = None
+        if on_chunk is not None:
+            def _cb(_user, chunk, data, n):
+                on_chunk(int(chunk), np.ctypeslib.as_array(data, shape=(int(n),)))
+            cb = self._CHUNK_CB(_cb)
+        _check(lib.cintx_plan_execute_host_ring(self.handle, ring.ctypes.data_as(_dp), ring.size,
+                                                ctypes.cast(cb, ctypes.c_void_p) if cb else None, None))
+        return ring
 
     def close(self):
         if self.handle:

@@ -511,6 +511,85 @@ int cintx_plan_execute_host(CintxPlan* p, int64_t chunk, double* out_host) {
   return CINTX_STATUS_SUCCESS;
 }
 
+int cintx_plan_execute_host_ring(CintxPlan* p, double* ring, int64_t ring_doubles,
+                                  void (*on_chunk)(void* user, int64_t chunk, const double* data, int64_t n),
+                                  void* user) {
+  clear_error();
+  if (!p || !ring) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and ring must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  const int64_t nch = (int64_t)p->chunks.size();
+  long long slot = 1;
+  for (const Chunk& c : p->chunks) slot = std::max(slot, c.out_size);
+  if (ring_doubles < 2 * slot) {
+    set_error(CINTX_STATUS_BUFFER_TOO_SMALL, "the host ring must hold two of the plan's largest chunks");
+    return CINTX_STATUS_BUFFER_TOO_SMALL;
+  }
+  if (!p->stream && cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  if (!p->copy_stream && cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaStreamCreate failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  for (int b = 0; b < 2; ++b) {
+    if ((!p->ev_done[b] && cudaEventCreateWithFlags(&p->ev_done[b], cudaEventDisableTiming) != cudaSuccess) ||
+        (!p->ev_free[b] && cudaEventCreateWithFlags(&p->ev_free[b], cudaEventDisableTiming) != cudaSuccess)) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaEventCreate failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+  }
+  if (2 * slot > p->stage_cap) {
+    if (p->d_stage) cudaFree(p->d_stage);
+    if (cudaMalloc(&p->d_stage, sizeof(double) * 2 * slot) != cudaSuccess) {
+      p->d_stage = nullptr;
+      p->stage_cap = 0;
+      set_error(CINTX_STATUS_ALLOCATION_FAILED, "device output staging allocation failed");
+      return CINTX_STATUS_ALLOCATION_FAILED;
+    }
+    p->stage_cap = 2 * slot;
+  }
+  // chunk c: evaluated into device stage c%2 (stream), copied to ring slot c%2 (copy stream);
+  // the host waits for chunk c-1's copy (while chunk c computes) and hands it to on_chunk before
+  // slot (c-1)%2 is written again by chunk c+1
+  int rc = CINTX_STATUS_SUCCESS;
+  auto host_wait = [&](int64_t c) -> bool {
+    if (cudaEventSynchronize(p->ev_free[c % 2]) != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "device execution failed");
+      return false;
+    }
+    if (on_chunk) on_chunk(user, c, ring + (size_t)(c % 2) * slot, p->chunks[c].out_size);
+    return true;
+  };
+  for (int64_t c = 0; c < nch; ++c) {
+    const int b = (int)(c % 2);
+    double* stage = p->d_stage + (size_t)b * slot;
+    if (c >= 2) cudaStreamWaitEvent(p->stream, p->ev_free[b], 0);  // chunk c-2's copy left the stage
+    if ((rc = cintx_plan_execute(p, c, stage, p->stream))) break;
+    cudaEventRecord(p->ev_done[b], p->stream);
+    if (c >= 1 && !host_wait(c - 1)) {
+      rc = CINTX_STATUS_EXECUTION_FAILED;
+      break;
+    }
+    cudaStreamWaitEvent(p->copy_stream, p->ev_done[b], 0);
+    cudaMemcpyAsync(ring + (size_t)b * slot, stage, sizeof(double) * p->chunks[c].out_size, cudaMemcpyDeviceToHost,
+                    p->copy_stream);
+    cudaEventRecord(p->ev_free[b], p->copy_stream);
+  }
+  if (!rc && nch > 0 && !host_wait(nch - 1)) rc = CINTX_STATUS_EXECUTION_FAILED;
+  cudaError_t e1 = cudaStreamSynchronize(p->stream);
+  cudaError_t e2 = cudaStreamSynchronize(p->copy_stream);
+  if (rc) return rc;
+  if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED,
+              std::string("device execution failed: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
 int cintx_plan_stats(const CintxPlan* p, CintxPlanStats* s) {
   if (!p || !s) return CINTX_STATUS_NULL_POINTER;
   *s = p->stats;

@@ -221,6 +221,15 @@ CINTX_API int cintx_plan_segment_lanes(const CintxPlan *plan, int64_t chunk, int
  * runs on a second stream while chunk c+1 is evaluated (two staging buffers); page-locked
  * out_host lets the copies overlap.  Synchronous. */
 CINTX_API int cintx_plan_execute_host(CintxPlan *plan, int64_t chunk, double *out_host);
+/* End to end for sweeps larger than host memory: every chunk is evaluated and copied into one of
+ * two slots of the host ring (ring_doubles >= 2 x the largest chunk; page-locked memory lets the
+ * copies overlap the next chunk's kernels), and on_chunk(user, chunk, data, n) (may be NULL) is
+ * called for each chunk in order, on the calling thread, before its slot is reused.
+ * Synchronous. */
+CINTX_API int cintx_plan_execute_host_ring(CintxPlan *plan, double *ring, int64_t ring_doubles,
+                                           void (*on_chunk)(void *user, int64_t chunk, const double *data,
+                                                            int64_t n),
+                                           void *user);
 CINTX_API void cintx_plan_destroy(CintxPlan *plan);
 
 /* ---- evaluation without device allocation ------------------------------------------------ */

@@ -194,6 +194,14 @@ def test_execute_host_all_chunks_back_to_back(cx):
         assert off == st.nintegrals
         with pytest.raises(ValueError):
             plan.execute_host(np.zeros(st.nintegrals - 1))
+        # the two-slot host ring hands every chunk over in order, each equal to the above
+        ring = torch.empty(2 * st.max_chunk_doubles, dtype=torch.float64, pin_memory=True).numpy()
+        got = []
+        plan.execute_host_ring(ring, on_chunk=lambda c, a: got.append((c, a.copy())))
+        assert [c for c, _ in got] == list(range(st.nchunks))
+        assert np.array_equal(np.concatenate([a for _, a in got]), host)
+        with pytest.raises(cx.CintxError):
+            plan.execute_host_ring(np.zeros(2 * st.max_chunk_doubles - 1))
         plan.close()
 
 
