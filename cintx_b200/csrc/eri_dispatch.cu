@@ -32,6 +32,12 @@ int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int varia
   return pick_threads(li, lj, lk, ll, variant_acc(variant));
 }
 
+int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
+  if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  const int s = pick_threads(li, lj, lk, ll, variant_acc(variant));
+  return s == 1 ? 1 : s * 1024 + variant_regs(variant);  // one-lane shapes take no register cap
+}
+
 bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant) {
   LaunchArgs a{};
   a.query = 1;

@@ -57,12 +57,15 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
   return s;
 }
 
-// Launch-shape variants the autotuner chooses between: the accumulator budget per lane
-// (variant 0 is the default shape, used by plans that are not autotuned).
-constexpr int kNumVariants = 3;
+// Launch-shape variants the autotuner chooses between: the accumulator budget per lane and the
+// register cap of multi-lane shapes (variant 0 is the default shape, used by plans that are not
+// autotuned).  A 255-register cap halves the resident blocks but removes the spills that the
+// 128-register cap forces on most d/f/g multi-lane classes.
+constexpr int kNumVariants = 4;
 __host__ __device__ constexpr int variant_acc(int v) { return v == 1 ? 48 : (v == 2 ? 12 : 24); }
+__host__ __device__ constexpr int variant_regs(int v) { return v == 1 || v == 3 ? 255 : 128; }
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -103,7 +106,7 @@ struct EriShape {
   static constexpr int BLOCK = S >= 128 ? S : 128;
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
   // multi-lane kernels (their stalls are latency bound and need warps)
-  static constexpr int MINB = S == 1 ? 1 : 65536 / (BLOCK * 128);
+  static constexpr int MINB = S == 1 ? 1 : (65536 / (BLOCK * REGS) > 0 ? 65536 / (BLOCK * REGS) : 1);
   static constexpr int Q = BLOCK / S;
   // one-lane classes of low order stage their root-table block in shared memory: the lanes'
   // scattered coefficient loads then cost shared-memory wavefronts instead of L1 sectors
@@ -380,14 +383,14 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
   }
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC>::BLOCK,
-                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC>::MINB)
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>::BLOCK,
+                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
                  double prim_eps) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];

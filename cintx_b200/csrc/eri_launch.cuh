@@ -35,11 +35,11 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 
 int device_sm_count();
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -81,14 +81,18 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
       constexpr int k = decltype(K)::value, l = decltype(L)::value;
       if constexpr (class_valid(LI, LJ, k, l)) {
         if (lk == k && ll == l) {
-          // variants that give the default lane count are not compiled separately
+          // variants that give the default shape (lanes, and for multi-lane shapes the register
+          // cap) are not compiled separately
           constexpr int s0 = pick_threads(LI, LJ, k, l, variant_acc(0));
           constexpr int s1 = pick_threads(LI, LJ, k, l, variant_acc(1));
           constexpr int s2 = pick_threads(LI, LJ, k, l, variant_acc(2));
           if (a.fp32) err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
           else if (!sph) err = launch_eri<LI, LJ, k, l, false>(a);
-          else if (a.variant == 1 && s1 != s0) err = launch_eri<LI, LJ, k, l, true, double, variant_acc(1)>(a);
+          else if (a.variant == 1 && s1 > 1)
+            err = launch_eri<LI, LJ, k, l, true, double, variant_acc(1), variant_regs(1)>(a);
           else if (a.variant == 2 && s2 != s0) err = launch_eri<LI, LJ, k, l, true, double, variant_acc(2)>(a);
+          else if (a.variant == 3 && s0 > 1)
+            err = launch_eri<LI, LJ, k, l, true, double, variant_acc(3), variant_regs(3)>(a);
           else err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }

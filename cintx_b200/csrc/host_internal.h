@@ -141,6 +141,8 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
 // Lanes per quartet of a launch-shape variant (0 = default shape); variants that do not apply
 // (cartesian or FP32 classes, unknown ids) report the default shape.
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-constexpr int kLaunchVariants = 3;
+// Distinct launch shape of a variant (lanes and register cap), for telling variants apart.
+int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
+constexpr int kLaunchVariants = 4;
 
 }  // namespace cintx

@@ -732,8 +732,9 @@ int cintx_plan_autotune(CintxPlan* p, int64_t chunk, double* out_dev, void* stre
     set_error(CINTX_STATUS_EXECUTION_FAILED, "cudaEventCreate failed");
     return CINTX_STATUS_EXECUTION_FAILED;
   }
-  // time every class segment of the chunk in each launch shape that gives a distinct lane
-  // count (and needs device scratch only if the default shape does, so graphs stay possible)
+  // time every class segment of the chunk in each launch shape that is distinct (lanes per
+  // quartet, register cap) and needs device scratch only if the default shape does, so graphs
+  // stay possible
   std::map<std::tuple<int, int, int, int, int>, int> best;
   for (const auto& tg : target) {
     const auto& key = tg.first;
@@ -743,9 +744,9 @@ int cintx_plan_autotune(CintxPlan* p, int64_t chunk, double* out_dev, void* stre
     double best_ms = 1e300;
     int best_v = 0;
     for (int v = 0; v < kLaunchVariants && !rc; ++v) {
-      const int lanes = variant_lanes(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, sg0.fp32, v);
-      if (std::find(lanes_seen.begin(), lanes_seen.end(), lanes) != lanes_seen.end()) continue;
-      lanes_seen.push_back(lanes);
+      const int shape = variant_shape(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, sg0.fp32, v);
+      if (std::find(lanes_seen.begin(), lanes_seen.end(), shape) != lanes_seen.end()) continue;
+      lanes_seen.push_back(shape);
       if (!scratch0 && class_needs_scratch(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, v)) continue;
       Segment sg = sg0;
       sg.variant = v;
