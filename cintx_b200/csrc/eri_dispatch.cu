@@ -29,13 +29,16 @@ static_assert(kNumVariants == kLaunchVariants, "variant count differs between ke
 
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   return pick_threads(li, lj, lk, ll, variant_acc(variant));
 }
 
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   const int s = pick_threads(li, lj, lk, ll, variant_acc(variant));
-  return s == 1 ? 1 : s * 1024 + variant_regs(variant);  // one-lane shapes take no register cap
+  if (s == 1) return 1;  // one-lane shapes take no register cap
+  return (variant_sliced(variant) ? 1 << 20 : 0) + s * 1024 + variant_regs(variant);
 }
 
 bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant) {

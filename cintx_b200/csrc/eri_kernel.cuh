@@ -61,11 +61,26 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // register cap of multi-lane shapes (variant 0 is the default shape, used by plans that are not
 // autotuned).  A 255-register cap halves the resident blocks but removes the spills that the
 // 128-register cap forces on most d/f/g multi-lane classes.
-constexpr int kNumVariants = 4;
-__host__ __device__ constexpr int variant_acc(int v) { return v == 1 ? 48 : (v == 2 ? 12 : 24); }
-__host__ __device__ constexpr int variant_regs(int v) { return v == 1 || v == 3 ? 255 : 128; }
+// Variants 4 and 5 ("sliced") run a multi-lane class without any barrier inside the primitive
+// loop: every lane evaluates the roots and all 3*NR recurrences itself in registers and
+// accumulates its own slice of (j,k,l) tuples (redundant FP64 work for no shared-memory
+// hand-offs); the lanes meet only for the cartesian-to-spherical stages.
+constexpr int kNumVariants = 6;
+__host__ __device__ constexpr int variant_acc(int v) {
+  return v == 1 || v == 5 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
+}
+__host__ __device__ constexpr int variant_regs(int v) { return v == 0 || v == 2 ? 128 : 255; }
+__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5; }
+// a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (each
+// lane's slice is a separate compile-time instance of the register path)
+__host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int v) {
+  return variant_sliced(v) && pick_threads(li, lj, lk, ll, variant_acc(v)) >= 2 &&
+         pick_threads(li, lj, lk, ll, variant_acc(v)) <= 4 &&
+         3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= (v == 4 ? 48 : 72);
+}
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
+          bool SLICE = false>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -101,7 +116,9 @@ struct EriShape {
   static constexpr int B_G = SM_G * (int)sizeof(R);
   static constexpr int B_SCR = SM_SCR * (int)sizeof(R);
   static constexpr int B_GROUP_RAW =
-      S == 1 ? 0 : cmax(B_ROOTS + B_G + B_SCR, GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8);
+      S == 1 ? 0
+             : (SLICE ? (GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8)
+                      : cmax(B_ROOTS + B_G + B_SCR, GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8));
   static constexpr int B_GROUP = (B_GROUP_RAW + 15) & ~15;
   static constexpr int BLOCK = S >= 128 ? S : 128;
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
@@ -299,7 +316,7 @@ struct TupleOffsets {
 // tiles), so the inner loop's primitive-pair loads are warp-wide broadcasts; the lane's (kl)
 // primitive pair is loaded once per outer iteration.  `tab` is the shared-memory copy of the
 // order-NR root table when SH::STAGE_TABLE (otherwise the global table is read).
-template <int LI, int LJ, int LK, int LL, class SH, class R>
+template <int LI, int LJ, int LK, int LL, class SH, class R, int SLICE = 0>
 __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const ShellPair& pkl,
                                                    const PrimPair* __restrict__ prims, const RysTable& rys,
                                                    const double* tab, double expcutoff, double prim_eps,
@@ -364,12 +381,15 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
           // every index below is a constant expression, so gg and acc stay in registers
           static_loop(std::make_integer_sequence<int, TPT * NFI>{}, [&](auto c) {
             constexpr int k = decltype(c)::value / NFI, fi = decltype(c)::value % NFI;
-            constexpr TupleOffsets<SH, LJ, LK, LL> TO{};
-            constexpr int ix = cart_x(LI, fi) + TO.ox[k];
-            constexpr int iy = GSZ + cart_y(LI, fi) + TO.oy[k];
-            constexpr int iz = 2 * GSZ + cart_z(LI, fi) + TO.oz[k];
-            if constexpr (std::is_same<R, double>::value) acc[k][fi] = fma(gg[ix] * gg[iy], gg[iz], acc[k][fi]);
-            else part[k][fi] = fmaf(gg[ix] * gg[iy], gg[iz], part[k][fi]);
+            constexpr int t = SLICE + SH::S * k;  // this lane's k-th (j,k,l) tuple
+            if constexpr (t < SH::NTUP) {
+              constexpr TupleOffsets<SH, LJ, LK, LL> TO{};
+              constexpr int ix = cart_x(LI, fi) + TO.ox[t];
+              constexpr int iy = GSZ + cart_y(LI, fi) + TO.oy[t];
+              constexpr int iz = 2 * GSZ + cart_z(LI, fi) + TO.oz[t];
+              if constexpr (std::is_same<R, double>::value) acc[k][fi] = fma(gg[ix] * gg[iy], gg[iz], acc[k][fi]);
+              else part[k][fi] = fmaf(gg[ix] * gg[iy], gg[iz], part[k][fi]);
+            }
           });
         }
         if constexpr (!std::is_same<R, double>::value) {
@@ -383,14 +403,15 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
   }
 }
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>::BLOCK,
-                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>::MINB)
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
+          bool SLICE = false>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>::BLOCK,
+                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
                  double prim_eps) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];
@@ -425,6 +446,13 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>::B
     if constexpr (S == 1) {
       prim_loop_one_lane<LI, LJ, LK, LL, SH, R>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff,
                                                 prim_eps, lt, acc);
+    } else if constexpr (SLICE) {
+      // each lane runs the register path for its own tuple slice (lane + S*k)
+      static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
+        if (lane == decltype(j)::value)
+          prim_loop_one_lane<LI, LJ, LK, LL, SH, R, decltype(j)::value>(pij, pkl, prims, rys, nullptr, expcutoff,
+                                                                         prim_eps, lt, acc);
+      });
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];

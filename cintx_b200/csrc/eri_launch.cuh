@@ -35,11 +35,12 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 
 int device_sm_count();
 
-template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128>
+template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
+          bool SLICE = false>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -86,14 +87,46 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
           constexpr int s0 = pick_threads(LI, LJ, k, l, variant_acc(0));
           constexpr int s1 = pick_threads(LI, LJ, k, l, variant_acc(1));
           constexpr int s2 = pick_threads(LI, LJ, k, l, variant_acc(2));
-          if (a.fp32) err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
-          else if (!sph) err = launch_eri<LI, LJ, k, l, false>(a);
-          else if (a.variant == 1 && s1 > 1)
-            err = launch_eri<LI, LJ, k, l, true, double, variant_acc(1), variant_regs(1)>(a);
-          else if (a.variant == 2 && s2 != s0) err = launch_eri<LI, LJ, k, l, true, double, variant_acc(2)>(a);
-          else if (a.variant == 3 && s0 > 1)
-            err = launch_eri<LI, LJ, k, l, true, double, variant_acc(3), variant_regs(3)>(a);
-          else err = launch_eri<LI, LJ, k, l, true>(a);
+          // only shapes that differ from the default are instantiated (if constexpr)
+          bool done = false;
+          if (a.fp32) {
+            err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
+            done = true;
+          } else if (!sph) {
+            err = launch_eri<LI, LJ, k, l, false>(a);
+            done = true;
+          }
+          if constexpr (s1 != s0 || s1 > 1) {
+            if (!done && a.variant == 1) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(1), variant_regs(1)>(a);
+              done = true;
+            }
+          }
+          if constexpr (s2 != s0) {
+            if (!done && a.variant == 2) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(2)>(a);
+              done = true;
+            }
+          }
+          if constexpr (s0 > 1) {
+            if (!done && a.variant == 3) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(3), variant_regs(3)>(a);
+              done = true;
+            }
+          }
+          if constexpr (sliced_ok(LI, LJ, k, l, 4)) {
+            if (!done && a.variant == 4) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(4), variant_regs(4), true>(a);
+              done = true;
+            }
+          }
+          if constexpr (sliced_ok(LI, LJ, k, l, 5)) {
+            if (!done && a.variant == 5) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(5), variant_regs(5), true>(a);
+              done = true;
+            }
+          }
+          if (!done) err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }
     });

@@ -143,6 +143,6 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
 // Distinct launch shape of a variant (lanes and register cap), for telling variants apart.
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-constexpr int kLaunchVariants = 4;
+constexpr int kLaunchVariants = 6;
 
 }  // namespace cintx
