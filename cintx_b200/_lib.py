@@ -106,6 +106,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_rysnet_loss_grad.restype = _i
     L.cintx_rysnet_train.argtypes = [_fp, _i64, _i, _i, _i, _i, ctypes.c_float, ctypes.c_uint64, _dp]
     L.cintx_rysnet_train.restype = _i
+    L.cintx_plan_use_learned_roots.argtypes = [_vp, _fp, _i64p, _i64p]
+    L.cintx_plan_use_learned_roots.restype = _i
     L.cintx_rys_learned_batch.argtypes = [_fp, _i, _dp, _i64, _i, _dp, _ip, _ip]
     L.cintx_rys_learned_batch.restype = _i
     L.cintx_fp64_fma_probe.argtypes = [_i, _i, _i, _vp, _vp]
@@ -325,6 +327,15 @@ class Plan:
         q = np.zeros((n, 4), dtype=np.int32)
         _check(lib.cintx_plan_sample_quartets(self.handle, seed, n, q.ctypes.data_as(_ip)))
         return q
+
+    def use_learned_roots(self, net: "RysNet | None"):
+        """Explicit plans: take Rys roots from the learned initializer + FP64 refinement (None:
+        the table again).  Returns (fallback count, primitive quartets)."""
+        fb = ctypes.c_int64()
+        npt = ctypes.c_int64()
+        params = None if net is None else net.params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        _check(lib.cintx_plan_use_learned_roots(self.handle, params, ctypes.byref(fb), ctypes.byref(npt)))
+        return fb.value, npt.value
 
     def execute(self, out_ptr: int, chunk: int = -1, stream: int = 0):
         """Asynchronous device execution into device pointer out_ptr."""

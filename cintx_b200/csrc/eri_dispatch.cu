@@ -7,7 +7,7 @@ namespace cintx {
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32,
-                         double prim_eps, int variant) {
+                         double prim_eps, int variant, const double* rootbuf, const long long* rootbase) {
   LaunchArgs a;
   a.recs = recs;
   a.nrec = nrec;
@@ -22,6 +22,8 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
   a.fp32 = fp32;
   a.prim_eps = prim_eps;
   a.variant = variant;
+  a.rootbuf = rootbuf;
+  a.rootbase = rootbase;
   return dispatch_eri(li, lj, lk, ll, sph, a);
 }
 

@@ -320,7 +320,8 @@ template <int LI, int LJ, int LK, int LL, class SH, class R, int SLICE = 0>
 __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const ShellPair& pkl,
                                                    const PrimPair* __restrict__ prims, const RysTable& rys,
                                                    const double* tab, double expcutoff, double prim_eps,
-                                                   const LaneTuples<SH>& lt, double (&acc)[SH::TPT][SH::NFI]) {
+                                                   const double* __restrict__ rb, const LaneTuples<SH>& lt,
+                                                   double (&acc)[SH::TPT][SH::NFI]) {
   constexpr int NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool SSSS = LI + LJ + LK + LL == 0;
   for (int b = 0; b < pkl.nprim; ++b) {
@@ -344,7 +345,14 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
       const double x = a1 * inv_aijkl * rr;
       const double fac = pi.kab * pk.kab * rs * inv_a1;
       double t2[NR], w[NR];
-      if constexpr (SH::STAGE_TABLE) {
+      if (rb) {  // roots precomputed for this primitive quartet (learned-root plans)
+        const double* r = rb + (size_t)(b * pij.nprim + a) * (2 * NR);
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+          t2[i] = r[i];
+          w[i] = r[NR + i];
+        }
+      } else if constexpr (SH::STAGE_TABLE) {
         if constexpr (SSSS) rys_all_staged<NR, NR, 2 * NR>(tab, rys, x, t2, w);
         else rys_all_staged<NR>(tab, rys, x, t2, w);
       } else {
@@ -410,7 +418,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
-                 double prim_eps) {
+                 double prim_eps, const double* __restrict__ rootbuf, const long long* __restrict__ rootbase) {
   using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
@@ -435,6 +443,8 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
 
   for (int q = blockIdx.x * SH::Q + group; q < nrec; q += gridDim.x * SH::Q) {
     const QuartetRec rec = recs[q];
+    // precomputed roots of this quartet's primitive quartets ([b][a][2*NR]), or table roots
+    const double* rb = rootbuf ? rootbuf + rootbase[q] : nullptr;
     const ShellPair pij = pairs[rec.pij];
     const ShellPair pkl = pairs[rec.pkl];
     double acc[TPT][NFI];
@@ -445,13 +455,13 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
 
     if constexpr (S == 1) {
       prim_loop_one_lane<LI, LJ, LK, LL, SH, R>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff,
-                                                prim_eps, lt, acc);
+                                                prim_eps, rb, lt, acc);
     } else if constexpr (SLICE) {
       // each lane runs the register path for its own tuple slice (lane + S*k)
       static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
         if (lane == decltype(j)::value)
           prim_loop_one_lane<LI, LJ, LK, LL, SH, R, decltype(j)::value>(pij, pkl, prims, rys, nullptr, expcutoff,
-                                                                         prim_eps, lt, acc);
+                                                                         prim_eps, rb, lt, acc);
       });
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
@@ -474,8 +484,11 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
         const double fac = pi.kab * pk.kab * rs * inv_a1;
         const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
 
-        // roots: the group's lanes split the 2*NR table polynomials
-        if constexpr (SH::STAGE_TABLE) {
+        // roots: the group's lanes split the 2*NR table polynomials (or copy precomputed ones)
+        if (rb) {
+          const double* r = rb + (size_t)(b * pij.nprim + a) * (2 * NR);
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = r[f];
+        } else if constexpr (SH::STAGE_TABLE) {
           for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
         } else {
           for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);

@@ -21,6 +21,8 @@ struct LaunchArgs {
   bool fp32 = false;  // FP32 recurrences and products (spherical output only)
   double prim_eps = 0;  // primitive Schwarz threshold (0: no primitive screening beyond libcint's)
   int variant = 0;      // launch-shape variant (spherical FP64 classes; see variant_acc)
+  const double* rootbuf = nullptr;     // precomputed roots [record's base + (b*npij + a)*2*NR]
+  const long long* rootbase = nullptr;  // per record of this launch: its base in rootbuf
 };
 
 // Device scratch for classes whose transform buffers live in global memory: returns a buffer
@@ -60,7 +62,8 @@ cudaError_t launch_eri(const LaunchArgs& a) {
     if (!scratch) return cudaErrorMemoryAllocation;
   }
   kern<<<(unsigned)blocks, SH::BLOCK, SH::SMEM_BYTES, a.stream>>>(a.recs, a.nrec, a.pairs, a.prims, a.out,
-                                                                   a.st, a.expcutoff, a.rys, scratch, a.prim_eps);
+                                                                   a.st, a.expcutoff, a.rys, scratch, a.prim_eps,
+                                                                   a.rootbuf, a.rootbase);
   return cudaGetLastError();
 }
 

@@ -137,7 +137,12 @@ bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant =
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32 = false,
-                         double prim_eps = 0.0, int variant = 0);
+                         double prim_eps = 0.0, int variant = 0, const double* rootbuf = nullptr,
+                         const long long* rootbase = nullptr);
+// Learned Rys roots (rysnet.cu) of order n at count device points: out[p*2n + f], status[p]
+// (0 refined, 1 table fallback, 2 closed form), asynchronous on stream.
+cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, const double* d_x, long long count,
+                             double* d_out, int* d_status, int* d_iters, cudaStream_t stream);
 // Lanes per quartet of a launch-shape variant (0 = default shape); variants that do not apply
 // (cartesian or FP32 classes, unknown ids) report the default shape.
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);

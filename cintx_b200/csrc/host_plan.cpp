@@ -27,6 +27,8 @@ cudaError_t launch_gen_tile(const int* rows, const int* cols, const long long* r
                             cudaStream_t stream);
 cudaError_t launch_gen_ranges(const GenRange* ranges, int nranges, long long nrec, QuartetRec* recs,
                               cudaStream_t stream);
+cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPair* pairs, const PrimPair* prims,
+                          const long long* pbase, double* xout, cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -104,6 +106,10 @@ struct CintxPlan {
   long long stage_cap = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;
+  // explicit plans with learned roots (cintx_plan_use_learned_roots): roots of every primitive
+  // quartet, and per record its base (doubles) in d_rootbuf
+  double* d_rootbuf = nullptr;
+  long long* d_rootbase = nullptr;
   cudaEvent_t ev_done[2] = {nullptr, nullptr};
   cudaEvent_t ev_free[2] = {nullptr, nullptr};
 };
@@ -136,6 +142,10 @@ void free_plan_device(CintxPlan* p) {
   p->stream = nullptr;
   if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   p->copy_stream = nullptr;
+  if (p->d_rootbuf) cudaFree(p->d_rootbuf);
+  if (p->d_rootbase) cudaFree(p->d_rootbase);
+  p->d_rootbuf = nullptr;
+  p->d_rootbase = nullptr;
   for (int b = 0; b < 2; ++b) {
     if (p->ev_done[b]) cudaEventDestroy(p->ev_done[b]);
     if (p->ev_free[b]) cudaEventDestroy(p->ev_free[b]);
@@ -386,9 +396,10 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
   // the kernels take an int count; split very large segments
   for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
     const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
+    const bool rb = p->d_rootbuf && sg.tile == -1;  // learned roots: explicit plans only
     cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
                                  out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps,
-                                 sg.variant);
+                                 sg.variant, rb ? p->d_rootbuf : nullptr, rb ? p->d_rootbase + sg.rec0 + r0 : nullptr);
     if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -587,6 +598,104 @@ int cintx_plan_execute_host_ring(CintxPlan* p, double* ring, int64_t ring_double
               std::string("device execution failed: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
     return CINTX_STATUS_EXECUTION_FAILED;
   }
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_use_learned_roots(CintxPlan* p, const float* params, int64_t* nfallback, int64_t* npoints) {
+  clear_error();
+  if (!p) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (p->d_rootbuf) cudaFree(p->d_rootbuf);
+  if (p->d_rootbase) cudaFree(p->d_rootbase);
+  p->d_rootbuf = nullptr;
+  p->d_rootbase = nullptr;
+  if (p->gexec) {  // the captured graph reads the table roots
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  if (!params) return CINTX_STATUS_SUCCESS;  // back to table roots
+  if (!p->tiles.empty() || p->chunks.size() != 1) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "learned roots are available for explicit tuple plans");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  DeviceState* ds;
+  int rc;
+  if ((rc = device_state(&ds))) return rc;
+  const Opt* o = p->opt;
+  const Chunk& ch = p->chunks[0];
+  // per record: its primitive quartets' base in points (within its segment) and in doubles
+  std::vector<long long> pbase(p->rec_capacity), dbase(p->rec_capacity);
+  std::vector<long long> seg_pts(ch.segs.size()), seg_dbl(ch.segs.size());
+  long long dtot = 0;
+  for (size_t si = 0; si < ch.segs.size(); ++si) {
+    const Segment& sg = ch.segs[si];
+    const int nr = (sg.li + sg.lj + sg.lk + sg.ll) / 2 + 1;
+    if (nr > 9) {
+      set_error(CINTX_STATUS_UNSUPPORTED_API, "learned roots cover 1..9 roots");
+      return CINTX_STATUS_UNSUPPORTED_API;
+    }
+    long long pts = 0;
+    seg_dbl[si] = dtot;
+    for (long long r = sg.rec0; r < sg.rec0 + sg.nrec; ++r) {
+      const QuartetRec& q = p->h_recs[r];
+      pbase[r] = pts;
+      dbase[r] = dtot + pts * 2 * nr;
+      pts += (long long)o->pair_nprim[q.pij] * o->pair_nprim[q.pkl];
+    }
+    seg_pts[si] = pts;
+    dtot += pts * 2 * nr;
+  }
+  long long maxpts = 1;
+  for (long long v : seg_pts) maxpts = std::max(maxpts, v);
+  float* d_params = nullptr;
+  long long* d_pbase = nullptr;
+  double* d_x = nullptr;
+  int *d_status = nullptr, *d_iters = nullptr;
+  bool ok = cudaMalloc(&p->d_rootbuf, sizeof(double) * std::max(dtot, 1LL)) == cudaSuccess &&
+            cudaMalloc(&p->d_rootbase, sizeof(long long) * std::max<long long>(p->rec_capacity, 1)) == cudaSuccess &&
+            cudaMalloc(&d_params, sizeof(float) * CINTX_RYSNET_NPARAM) == cudaSuccess &&
+            cudaMalloc(&d_pbase, sizeof(long long) * std::max<long long>(p->rec_capacity, 1)) == cudaSuccess &&
+            cudaMalloc(&d_x, sizeof(double) * maxpts) == cudaSuccess &&
+            cudaMalloc(&d_status, sizeof(int) * maxpts) == cudaSuccess &&
+            cudaMalloc(&d_iters, sizeof(int) * maxpts) == cudaSuccess;
+  int64_t fb = 0, total = 0;
+  if (ok) {
+    cudaMemcpy(p->d_rootbase, dbase.data(), sizeof(long long) * dbase.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_pbase, pbase.data(), sizeof(long long) * pbase.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_params, params, sizeof(float) * CINTX_RYSNET_NPARAM, cudaMemcpyHostToDevice);
+    std::vector<int> st;
+    for (size_t si = 0; si < ch.segs.size() && ok; ++si) {
+      const Segment& sg = ch.segs[si];
+      const int nr = (sg.li + sg.lj + sg.lk + sg.ll) / 2 + 1;
+      if (!seg_pts[si]) continue;
+      ok = launch_prim_x(p->d_recs + sg.rec0, sg.nrec, o->d_pairs, o->d_prims, d_pbase + sg.rec0, d_x, 0) ==
+               cudaSuccess &&
+           rys_learned_eval(d_params, ds->rys, nr, d_x, seg_pts[si], p->d_rootbuf + seg_dbl[si], d_status, d_iters,
+                            0) == cudaSuccess &&
+           cudaDeviceSynchronize() == cudaSuccess;
+      st.resize(seg_pts[si]);
+      if (ok) cudaMemcpy(st.data(), d_status, sizeof(int) * seg_pts[si], cudaMemcpyDeviceToHost);
+      for (int v : st) fb += v == 1;
+      total += seg_pts[si];
+    }
+  }
+  cudaFree(d_params);
+  cudaFree(d_pbase);
+  cudaFree(d_x);
+  cudaFree(d_status);
+  cudaFree(d_iters);
+  if (!ok) {
+    if (p->d_rootbuf) cudaFree(p->d_rootbuf);
+    if (p->d_rootbase) cudaFree(p->d_rootbase);
+    p->d_rootbuf = nullptr;
+    p->d_rootbase = nullptr;
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "learned root evaluation failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
+  if (nfallback) *nfallback = fb;
+  if (npoints) *npoints = total;
   return CINTX_STATUS_SUCCESS;
 }
 

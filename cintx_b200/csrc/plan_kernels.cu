@@ -72,7 +72,41 @@ __global__ void gen_range_quartets(const GenRange* __restrict__ ranges, int nran
   }
 }
 
+// x = a_ij a_kl / (a_ij + a_kl) |P - Q|^2 of every primitive quartet (b over the (kl) pair's
+// primitives, a over the (ij) pair's, the ERI kernels' loop order) of nrec records, written at
+// xout[pbase[r] + b * npij + a]; the same expression as the kernels, so the roots computed from
+// it are the ones those kernels would evaluate.
+__global__ void prim_x_kernel(const QuartetRec* __restrict__ recs, long long nrec, const ShellPair* __restrict__ pairs,
+                              const PrimPair* __restrict__ prims, const long long* __restrict__ pbase,
+                              double* __restrict__ xout) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nrec;
+       r += (long long)gridDim.x * blockDim.x) {
+    const QuartetRec rec = recs[r];
+    const ShellPair pij = pairs[rec.pij], pkl = pairs[rec.pkl];
+    for (int b = 0; b < pkl.nprim; ++b) {
+      const PrimPair pk = prims[pkl.prim_off + b];
+      for (int a = 0; a < pij.nprim; ++a) {
+        const PrimPair pi = prims[pij.prim_off + a];
+        const double aijkl = pi.aij + pk.aij;
+        const double rs = rsqrt(aijkl);
+        const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
+        xout[pbase[r] + (long long)b * pij.nprim + a] =
+            pi.aij * pk.aij * (rs * rs) * (pqx * pqx + pqy * pqy + pqz * pqz);
+      }
+    }
+  }
+}
+
 namespace cintx {
+cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPair* pairs, const PrimPair* prims,
+                          const long long* pbase, double* xout, cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec + 127) / 128;
+  if (blocks > 65535) blocks = 65535;
+  prim_x_kernel<<<(unsigned)blocks, 128, 0, stream>>>(recs, nrec, pairs, prims, pbase, xout);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gen_ranges(const GenRange* ranges, int nranges, long long nrec, QuartetRec* recs,
                               cudaStream_t stream) {
   if (nrec <= 0) return cudaSuccess;

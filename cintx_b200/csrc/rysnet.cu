@@ -392,6 +392,15 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) rys_learned_kernel(const floa
   }
 }
 
+cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, const double* d_x, long long count,
+                             double* d_out, int* d_status, int* d_iters, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((count + EVAL_WARPS - 1) / EVAL_WARPS, 148LL * 16);
+  rys_learned_kernel<<<(unsigned)blocks, 32 * EVAL_WARPS, 0, stream>>>(d_params, rys, n, d_x, count, 0, d_out,
+                                                                       d_status, d_iters);
+  return cudaGetLastError();
+}
+
 }  // namespace cintx
 
 using namespace cintx;

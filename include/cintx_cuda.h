@@ -297,6 +297,14 @@ CINTX_API int cintx_rysnet_train(float *params, int64_t nsamples, int n_lo, int 
  * (closed form).  iters[p]: Newton steps of the slowest root.  Synchronous. */
 CINTX_API int cintx_rys_learned_batch(const float *params, int nroots, const double *x, int64_t count, int mode,
                                       double *t2w, int *status, int *iters);
+/* Makes an explicit plan (cintx_plan_shells) take its Rys roots from RysNet (params on the host)
+ * instead of the table: the x of every primitive quartet is enumerated on the device, its roots
+ * are computed by the refinement of cintx_rys_learned_batch (mode 0, table fallback per point)
+ * into a device buffer the ERI kernels read.  *nfallback / *npoints (may be NULL) receive the
+ * fallback count and the number of primitive quartets.  params == NULL restores table roots.
+ * Synchronous; a graph captured earlier is released. */
+CINTX_API int cintx_plan_use_learned_roots(CintxPlan *plan, const float *params, int64_t *nfallback,
+                                           int64_t *npoints);
 
 /* FP64 FMA throughput probe (measurement only): blocks x threads threads each run
  * iters*16*8 FMAs and write one double to out_dev[blocks*threads].  Asynchronous on stream. */

@@ -85,3 +85,46 @@ def test_network_gain_over_refinement_without_it(cx, trained):
         for mode in (0, 1):
             fb[mode] += int((net.roots(n, x, mode=mode)[2] == 1).sum())
     assert fb[0] <= 0.002 * total and fb[1] >= 10 * max(fb[0], 1), fb
+
+
+def _g_quartets(mol, n, seed):
+    """Seeded quartets containing a g shell whose class needs 5..9 roots (sum of l >= 8)."""
+    rng = np.random.default_rng(seed)
+    ls = mol.bas[:, 1]
+    g = np.where(ls == 4)[0]
+    out = []
+    while len(out) < n:
+        q = rng.integers(0, mol.nbas, size=4)
+        q[rng.integers(0, 4)] = rng.choice(g)
+        if ls[q].sum() >= 8:
+            out.append(q)
+    return np.array(out, dtype=np.int32)
+
+
+def test_learned_roots_feed_the_integrals(cx, trained):
+    """g-shell int2e quartets evaluated by the ERI kernels with roots from the learned
+    initializer + refinement, against the same kernels with table roots and against libcint."""
+    from conftest import close
+    from cintx_b200 import molecules as M
+    from oracle import RefLibcint
+    net, _ = trained
+    mol = M.mol20_g()
+    quartets = _g_quartets(mol, 400, 31)
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        p_tab = cx.Plan.shells(opt, cx.INT2E, quartets)
+        out_tab = p_tab.execute_host(np.zeros(p_tab.stats.nintegrals))
+        p_lrn = cx.Plan.shells(opt, cx.INT2E, quartets)
+        fb, npt = p_lrn.use_learned_roots(net)
+        out_lrn = p_lrn.execute_host(np.zeros(p_lrn.stats.nintegrals))
+        assert npt > 0 and fb <= 0.01 * npt, (fb, npt)
+        assert close(out_lrn, out_tab), np.abs(out_lrn - out_tab).max()
+        assert p_lrn.use_learned_roots(None) == (0, 0)  # back to the table: identical output
+        assert np.array_equal(p_lrn.execute_host(np.zeros(p_lrn.stats.nintegrals)), out_tab)
+        offs = p_lrn.offsets
+        if RefLibcint.available():
+            ref = RefLibcint()
+            for k in range(0, len(quartets), 8):
+                r, _ = ref.int2e(quartets[k], mol)
+                assert close(out_lrn[offs[k]:offs[k] + r.size], r), quartets[k]
+        p_tab.close()
+        p_lrn.close()
