@@ -71,7 +71,8 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="mol120_spdf", choices=sorted(WORKLOADS) + sorted(DF_WORKLOADS))
+    ap.add_argument("--workload", default="mol120_spdf",
+                    choices=sorted(WORKLOADS) + sorted(DF_WORKLOADS) + ["mol20_g_learned"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk-doubles", type=int, default=1 << 28)
     ap.add_argument("--branches", type=int, default=4)
@@ -813,10 +814,124 @@ def df_arm(args):
     opt.close()
 
 
+def g_quartets(mol, n, seed):
+    """Seeded shell quartets containing a g shell whose class needs 5..9 Rys roots."""
+    rng = np.random.default_rng(seed)
+    ls = mol.bas[:, 1]
+    g = np.where(ls == 4)[0]
+    q = rng.integers(0, mol.nbas, size=(4 * n, 4))
+    q[np.arange(len(q)), rng.integers(0, 4, len(q))] = rng.choice(g, len(q))
+    q = q[ls[q].sum(axis=1) >= 8][:n]
+    return np.ascontiguousarray(q, dtype=np.int32)
+
+
+def learned_arm(args):
+    """the learned Rys-root initializer, trained on the device, its roots on 5e6
+    (x, n) points of the configs' distribution, and g-shell int2e quartets evaluated with learned
+    roots against the same kernels with table roots."""
+    import torch
+
+    import cintx_b200 as cx
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    mol = M.mol20_g()
+    net = cx.RysNet(seed=0)
+    t0 = time.perf_counter()
+    hist = net.train(nsamples=5_000_000, n_lo=5, n_hi=9, epochs=40, batch=16384, lr=3e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    # roots: 5e6 points, n uniform in 5..9, x 70% log-uniform [1e-7, 50], 30% uniform [50, 3000]
+    rng = np.random.default_rng(3)
+    npts = 5_000_000
+    nn = rng.integers(5, 10, npts)
+    x = np.where(rng.random(npts) < 0.7, np.exp(rng.uniform(np.log(1e-7), np.log(50.0), npts)),
+                 rng.uniform(50.0, 3000.0, npts))
+    worst, nfb, nref, ncl, iters = 0.0, 0, 0, 0, []
+    t_roots = 0.0
+    for n in range(5, 10):
+        sel = x[nn == n]
+        t1 = time.perf_counter()
+        t2, w, st, it = net.roots(n, sel)
+        t_roots += time.perf_counter() - t1
+        tt2, tw = cx.rys_t2_batch(n, sel)
+        ok = st == 0
+        if ok.any():
+            worst = max(worst, float(np.abs(t2[ok] / tt2[ok] - 1).max()), float(np.abs(w[ok] / tw[ok] - 1).max()))
+        nfb += int((st == 1).sum())
+        nref += int(ok.sum())
+        ncl += int((st == 2).sum())
+        iters.append(it[ok])
+    # integrals: quartets of the Schwarz-screened set (bound >= 1e-12) with a g shell and 5..9 roots
+    opt = cx.Optimizer(mol.atm, mol.bas, mol.env)
+    scr = cx.Plan.screened(opt, SCHWARZ, sph=True)
+    cand = scr.sample_quartets(2_000_000, 4)
+    scr.close()
+    ls = mol.bas[:, 1]
+    cand = cand[(ls[cand] == 4).any(axis=1) & (ls[cand].sum(axis=1) >= 8)]
+    quartets = np.ascontiguousarray(np.unique(cand, axis=0)[:100_000], dtype=np.int32)
+    p_tab = cx.Plan.shells(opt, cx.INT2E, quartets)
+    p_lrn = cx.Plan.shells(opt, cx.INT2E, quartets)
+    fb, npq = p_lrn.use_learned_roots(net)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    run_l = timed_multi(cx, torch, [(p_lrn, [0])], args, stream, 0, 1, tune=False)
+    run_t = timed_multi(cx, torch, [(p_tab, [0])], args, stream, 0, 1, tune=False)
+    nint = p_lrn.stats.nintegrals
+    a, b = run_l["rings"][0], run_t["rings"][0]
+    p_lrn.execute(a.data_ptr(), stream=stream.cuda_stream)
+    p_tab.execute(b.data_ptr(), stream=stream.cuda_stream)
+    stream.synchronize()
+    d = (a[:nint] - b[:nint]).abs()
+    diff = float(d.max())
+    big = b[:nint].abs() > 1e-6
+    rel = float((d[big] / b[:nint][big].abs()).max()) if bool(big.any()) else 0.0
+    parity = bool(((d <= 1e-12) | (d <= 1e-10 * b[:nint].abs())).all())
+    line = {"metric": "int2e_sph Gint/s on g-shell quartets with learned Rys roots (5..9 roots)",
+            "value": nint / (run_l["ms"] * 1e-3) / 1e9, "unit": "Gint/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": run_l["ms"], "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded molecule and root test set)",
+            "config": {"workload": args.workload, "nquartets": int(len(quartets)), "nintegrals": int(nint),
+                       "description": "mol20_g: up to 100000 distinct quartets of the Schwarz-screened set (1e-12) with "
+                                      "a g shell and 5..9 roots; "
+                                      "root test set 5e6 (x, n) points, n 5..9, x 70% log-uniform [1e-7, 50] "
+                                      "and 30% uniform [50, 3000]"},
+            "gpu_launches": run_l["launches"], "clocks": run_l["clocks"],
+            "table_roots": {"value": nint / (run_t["ms"] * 1e-3) / 1e9, "ms_per_step": run_t["ms"]},
+            "learned_roots": {"train_seconds": train_s, "train_samples": 5_000_000, "epochs": 40,
+                              "loss_first_last": [float(hist[0]), float(hist[-1])],
+                              "root_points": npts, "refined": nref, "fallback": nfb, "closed_form": ncl,
+                              "fallback_rate_in_table_range": nfb / max(nref + nfb, 1),
+                              "max_rel_err_vs_table": worst,
+                              "newton_steps_mean": float(np.concatenate(iters).mean()),
+                              "roots_per_s": npts / t_roots,
+                              "integral_primitive_quartets": int(npq), "integral_fallback": int(fb),
+                              "integral_max_abs_vs_table_roots": diff,
+                              "integral_max_rel_vs_table_roots": rel,
+                              "integral_parity_rule_vs_table_roots": parity}}
+    if os.path.exists(REF_DRIVER) and not args.no_cpu:
+        nq = min(20000, len(quartets))
+        r = run_libcint(mol, quartets[:nq], os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": r["nintegrals"] / r["seconds"] / 1e9, "unit": "Gint/s",
+                                "cores": int(r["threads"]), "kind": "reference",
+                                "sample": "the first %d of the quartets, libcint int2e_sph, OpenMP dynamic" % nq}
+    print(json.dumps(line))
+    p_tab.close()
+    p_lrn.close()
+    opt.close()
+
+
 def main():
     args = parse()
     df = args.workload in DF_WORKLOADS
-    if args.impl == "reference":
+    if args.workload == "mol20_g_learned":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the learned-root workload has no reference "
+                              "counterpart (libcint computes roots by its own fits); its cpu_baseline times libcint "
+                              "on the same quartets"}))
+        else:
+            learned_arm(args)
+    elif args.impl == "reference":
         (df_reference_arm if df else reference_arm)(args)
     else:
         (df_arm if df else our_arm)(args)
