@@ -29,6 +29,8 @@ cudaError_t launch_gen_ranges(const GenRange* ranges, int nranges, long long nre
                               cudaStream_t stream);
 cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPair* pairs, const PrimPair* prims,
                           const long long* pbase, double* xout, cudaStream_t stream);
+cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, const double* out, const long long* len,
+                                     double* q, cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -36,6 +38,7 @@ using namespace cintx;
 namespace {
 
 int nsph_or_cart(int l, bool sph) { return sph ? 2 * l + 1 : (l + 1) * (l + 2) / 2; }
+int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 struct Segment {
   int li, lj, lk, ll;
@@ -1062,71 +1065,96 @@ int compute_prim_schwarz(Opt* o) {
   std::lock_guard<std::mutex> lk(o->mu);
   if (o->prim_schwarz) return CINTX_STATUS_SUCCESS;
   const Basis& B = o->basis;
-  std::vector<int> pbase(B.nbas);
-  std::vector<int> bas;
-  std::vector<double> env = B.env;
-  env[PTR_EXPCUTOFF] = 1e6;  // keep every primitive pair: zero blocks must mean zero
-  int np = 0;
-  for (int sh = 0; sh < B.nbas; ++sh) {
-    const ShellInfo& S = B.sh[sh];
-    pbase[sh] = np;
-    for (int p = 0; p < S.nprim; ++p, ++np) {
-      const int pe = (int)env.size();
-      env.push_back(S.exps[p]);
-      const int pc = (int)env.size();
-      env.push_back(1.0);
-      const int row[8] = {S.atom, S.l, 1, 1, 0, pe, pc, 0};
-      bas.insert(bas.end(), row, row + 8);
-    }
-  }
-  // distinct primitive-shell pairs used by the stored primitive pairs (regular pairs only)
-  std::map<std::pair<int, int>, int> need;
-  std::vector<int> tuples;
-  std::vector<int> which(o->h_prims.size(), -1);
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc;
+  if ((rc = device_state(&ds)) || (rc = thread_scratch(&ts, 0, 0))) return rc;
   std::vector<ShellPair> sps(o->npairs + B.nvirt);
   cudaMemcpy(sps.data(), o->d_pairs, sizeof(ShellPair) * sps.size(), cudaMemcpyDeviceToHost);
-  for (int id = 0; id < o->npairs; ++id) {
-    const int sa = B.vshell[o->pair_a[id]], sb = B.vshell[o->pair_b[id]];
-    for (int k = sps[id].prim_off; k < sps[id].prim_off + sps[id].nprim; ++k) {
-      const int u = pbase[sa] + o->h_prim_a[k], v = pbase[sb] + o->h_prim_b[k];
-      auto key = std::make_pair(u, v);
-      auto it = need.find(key);
-      if (it == need.end()) {
-        it = need.emplace(key, (int)(tuples.size() / 4)).first;
-        const int t[4] = {u, v, u, v};
-        tuples.insert(tuples.end(), t, t + 4);
+  // One single-primitive copy of its shell pair per stored primitive pair k (regular pairs): the
+  // diagonal quartet of that copy is (c_a c_b)^2 (ab|ab) of the unit-coefficient primitives, since
+  // the pair prefactor holds the coefficients, so sqrt(max |block|) is q_k directly.  Cartesian
+  // blocks, no exponent screening; grouped by class (la, lb | la, lb).
+  long long nk = 0;
+  for (int id = 0; id < o->npairs; ++id) nk += sps[id].nprim;
+  std::vector<double> qk(nk, 0.0);
+  if (nk > 0) {
+    std::vector<ShellPair> tp(nk);
+    std::map<std::pair<int, int>, std::vector<QuartetRec>> groups;
+    std::vector<long long> blk_off, blk_len;  // per group record, in group order later
+    for (int id = 0; id < o->npairs; ++id)
+      for (int i = 0; i < sps[id].nprim; ++i) {
+        const long long k = sps[id].prim_off + i;
+        tp[k] = sps[id];
+        tp[k].prim_off = (int)k;
+        tp[k].nprim = 1;
+        QuartetRec r;
+        r.pij = r.pkl = (int)k;
+        r.out = 0;
+        groups[std::make_pair(o->pair_la[id], o->pair_lb[id])].push_back(r);
       }
-      which[k] = it->second;
+    // output offsets, block lengths and the record -> primitive-pair map, group by group
+    std::vector<QuartetRec> recs;
+    std::vector<long long> len;
+    long long tot = 0;
+    for (auto& kv : groups) {
+      const int la = kv.first.first, lb = kv.first.second;
+      const long long n = (long long)ncart(la) * ncart(la) * ncart(lb) * ncart(lb);
+      for (QuartetRec& r : kv.second) {
+        r.out = tot;
+        tot += n;
+        recs.push_back(r);
+        len.push_back(n);
+      }
     }
-  }
-  const int64_t nt = (int64_t)tuples.size() / 4;
-  std::vector<double> qprim(nt, 0.0);
-  if (nt > 0) {
-    Opt po;
-    po.magic = Opt::kMagic;
-    int rc = build_opt(&po, B.atm.data(), B.natm, bas.data(), np, env.data());
-    if (rc) return rc;
-    CintxPlan* pp = nullptr;
-    std::vector<int64_t> offs(nt);
-    rc = cintx_plan_shells(&pp, reinterpret_cast<CINTOpt*>(&po), CINTX_INT2E, tuples.data(), nt, 0, offs.data());
-    if (!rc) {
-      std::vector<double> outv(std::max<int64_t>(pp->stats.nintegrals, 1));
-      rc = cintx_plan_execute_host(pp, 0, outv.data());
-      const int64_t tot = pp->stats.nintegrals;
-      cintx_plan_destroy(pp);
-      if (!rc) {
-        for (int64_t t = 0; t < nt; ++t) {
-          const int64_t e1 = t + 1 < nt ? offs[t + 1] : tot;
-          double m = 0;
-          for (int64_t e = offs[t]; e < e1; ++e) m = std::max(m, fabs(outv[e]));
-          qprim[t] = sqrt(m);
+    ShellPair* d_tp = nullptr;
+    QuartetRec* d_recs = nullptr;
+    double* d_out = nullptr;
+    long long* d_len = nullptr;
+    double* d_q = nullptr;
+    bool ok = cudaMalloc(&d_tp, sizeof(ShellPair) * nk) == cudaSuccess &&
+              cudaMalloc(&d_recs, sizeof(QuartetRec) * recs.size()) == cudaSuccess &&
+              cudaMalloc(&d_out, sizeof(double) * std::max(tot, 1LL)) == cudaSuccess &&
+              cudaMalloc(&d_len, sizeof(long long) * len.size()) == cudaSuccess &&
+              cudaMalloc(&d_q, sizeof(double) * recs.size()) == cudaSuccess;
+    if (ok) {
+      cudaMemcpyAsync(d_tp, tp.data(), sizeof(ShellPair) * nk, cudaMemcpyHostToDevice, ts->stream);
+      cudaMemcpyAsync(d_recs, recs.data(), sizeof(QuartetRec) * recs.size(), cudaMemcpyHostToDevice, ts->stream);
+      cudaMemcpyAsync(d_len, len.data(), sizeof(long long) * len.size(), cudaMemcpyHostToDevice, ts->stream);
+      long long r0 = 0;
+      for (auto& kv : groups) {
+        const int la = kv.first.first, lb = kv.first.second;
+        const long long nrec = (long long)kv.second.size();
+        OutStrides st;
+        st.s0 = 1;
+        st.s1 = ncart(la);
+        st.s2 = (long long)ncart(la) * ncart(lb);
+        st.s3 = st.s2 * ncart(la);
+        for (long long q0 = 0; q0 < nrec && ok; q0 += 1LL << 30) {
+          const int nr = (int)std::min<long long>(nrec - q0, 1LL << 30);
+          ok = launch_class(la, lb, la, lb, false, d_recs + r0 + q0, nr, d_tp, o->d_prims, d_out, st, 1e6, ds->rys,
+                            ts->stream) == cudaSuccess;
+          ts->launches++;
         }
+        r0 += nrec;
       }
+      ok = ok && launch_block_absmax_sqrt(d_recs, (long long)recs.size(), d_out, d_len, d_q, ts->stream) == cudaSuccess;
+      std::vector<double> q(recs.size());
+      if (ok) ok = cudaMemcpyAsync(q.data(), d_q, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, ts->stream) ==
+                       cudaSuccess &&
+                   cudaStreamSynchronize(ts->stream) == cudaSuccess;
+      if (ok)
+        for (size_t i = 0; i < recs.size(); ++i) qk[recs[i].pij] = q[i];
     }
-    if (po.d_pairs) cudaFree(po.d_pairs);
-    if (po.d_prims) cudaFree(po.d_prims);
-    po.magic = 0;
-    if (rc) return rc;
+    cudaFree(d_tp);
+    cudaFree(d_recs);
+    cudaFree(d_out);
+    cudaFree(d_len);
+    cudaFree(d_q);
+    if (!ok) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "primitive Schwarz pass failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
   }
   // q per stored primitive pair, sorted by decreasing q within each shell pair
   o->pair_qp.assign(o->npairs + B.nvirt, 0.0);
@@ -1135,15 +1163,13 @@ int compute_prim_schwarz(Opt* o) {
     const int a = o->pair_a[id], b = o->pair_b[id];
     const ShellInfo& SA = B.sh[B.vshell[a]];
     const ShellInfo& SB = B.sh[B.vshell[b]];
-    const int ca = B.vctr[a], cb = B.vctr[b];
     const int k0 = sps[id].prim_off, n = sps[id].nprim;
     std::vector<int> ord(n);
     std::vector<double> qv(n);
     double sum = 0, amp = 1.0;
     for (int i = 0; i < n; ++i) {
       const int k = k0 + i;
-      const double cab = fabs(SA.coef[(size_t)ca * SA.nprim + o->h_prim_a[k]] * SB.coef[(size_t)cb * SB.nprim + o->h_prim_b[k]]);
-      qv[i] = cab * qprim[which[k]];
+      qv[i] = qk[k];
       ord[i] = i;
       sum += qv[i];
       const PrimPair& pp = o->h_prims[k];

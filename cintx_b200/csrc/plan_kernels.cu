@@ -97,6 +97,21 @@ __global__ void prim_x_kernel(const QuartetRec* __restrict__ recs, long long nre
   }
 }
 
+// q[r] = sqrt(max |out[recs[r].out .. + len[r])|): one warp per record.
+__global__ void block_absmax_sqrt_kernel(const QuartetRec* __restrict__ recs, long long nrec,
+                                         const double* __restrict__ out, const long long* __restrict__ len,
+                                         double* __restrict__ q) {
+  const int lane = threadIdx.x & 31;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nrec;
+       r += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const double* o = out + recs[r].out;
+    double m = 0.0;
+    for (long long e = lane; e < len[r]; e += 32) m = fmax(m, fabs(o[e]));
+    for (int s = 16; s > 0; s >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, s));
+    if (lane == 0) q[r] = sqrt(m);
+  }
+}
+
 namespace cintx {
 cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPair* pairs, const PrimPair* prims,
                           const long long* pbase, double* xout, cudaStream_t stream) {
@@ -104,6 +119,15 @@ cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPai
   long long blocks = (nrec + 127) / 128;
   if (blocks > 65535) blocks = 65535;
   prim_x_kernel<<<(unsigned)blocks, 128, 0, stream>>>(recs, nrec, pairs, prims, pbase, xout);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, const double* out, const long long* len,
+                                     double* q, cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec * 32 + 255) / 256;
+  if (blocks > 65535) blocks = 65535;
+  block_absmax_sqrt_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, out, len, q);
   return cudaGetLastError();
 }
 
