@@ -60,6 +60,11 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_int2e_screened.restype = _i
     L.cintx_plan_int2e_screened_mixed.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64, _d, _d]
     L.cintx_plan_int2e_screened_mixed.restype = _i
+    _sz = ctypes.c_size_t
+    L.cintrs_query_workspace.argtypes = [_i, _ip, _sz, _ip, _sz, _ip, _sz, _ip, _sz, _dp, _sz, _vp, _vp]
+    L.cintrs_query_workspace.restype = _i
+    L.cintrs_eval.argtypes = [_i, _dp, _sz, _ip, _sz, _ip, _sz, _ip, _sz, _ip, _sz, _dp, _sz, _vp, _dp, _sz, _vp]
+    L.cintrs_eval.restype = _i
     L.cintx_optimizer_pair_shells.argtypes = [ctypes.POINTER(_vp), _ip, _i, _ip, _i, _dp, _i]
     L.cintx_optimizer_pair_shells.restype = _i
     L.cintx_plan_int3c2e_screened.argtypes = [ctypes.POINTER(_vp), _vp, _d, _i, _i64, _i]

@@ -712,6 +712,135 @@ int int2c2e_cart(double* out, int* dims, int* shls, int* atm, int natm, int* bas
   return eval_call(F2C, false, out, dims, shls, atm, natm, bas, nbas, env, opt);
 }
 
+// cintx-capi's id-dispatch surface (crates/cintx-capi/src/shim.rs:312-453) for the Coulomb ids this
+// library computes: 9 int2e_cart, 10 int2e_sph, 12 int2c2e_cart, 13 int2c2e_sph.
+static int dispatch_prepare(int api, const int* dims, size_t dims_len, const int* shls, size_t shls_len,
+                            const int* atm, size_t atm_len, const int* bas, size_t bas_len, const double* env,
+                            size_t env_len, int* family, bool* sph, long long* nout) {
+  switch (api) {
+    case 9: *family = F2E; *sph = false; break;
+    case 10: *family = F2E; *sph = true; break;
+    case 12: *family = F2C; *sph = false; break;
+    case 13: *family = F2C; *sph = true; break;
+    default:
+      set_error(CINTX_STATUS_UNSUPPORTED_API, "api id " + std::to_string(api) +
+                                                  " is not a Coulomb integral this library computes (9, 10, 12, 13)");
+      return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (!shls || !atm || !bas || !env) {
+    set_error(CINTX_STATUS_NULL_POINTER, "shls, atm, bas and env must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  const int nsh = *family == F2E ? 4 : 2;
+  const long long natm = (long long)(atm_len / ATM_SLOTS), nbas = (long long)(bas_len / BAS_SLOTS);
+  if ((long long)shls_len < nsh || natm < 1 || nbas < 1) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "shls, atm or bas is too short");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  // every env slot the basis references must lie inside env_len
+  for (long long a = 0; a < natm; ++a)
+    if (atm[a * ATM_SLOTS + PTR_COORD] < 0 || (size_t)atm[a * ATM_SLOTS + PTR_COORD] + 3 > env_len) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "atm coordinates point outside env");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+  for (long long b = 0; b < nbas; ++b) {
+    const int* r = bas + b * BAS_SLOTS;
+    if (r[NPRIM_OF] < 1 || r[NCTR_OF] < 1 || r[PTR_EXP] < 0 || r[PTR_COEFF] < 0 ||
+        (size_t)r[PTR_EXP] + r[NPRIM_OF] > env_len || (size_t)r[PTR_COEFF] + (size_t)r[NPRIM_OF] * r[NCTR_OF] > env_len ||
+        r[ATOM_OF] < 0 || r[ATOM_OF] >= natm) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "bas row " + std::to_string(b) + " points outside env or atm");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+  }
+  long long n = 1;
+  std::vector<int> ext;
+  for (int a = 0; a < nsh; ++a) {
+    const int sh = shls[a];
+    if (sh < 0 || sh >= nbas) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "shell index out of range");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+    const int l = bas[sh * BAS_SLOTS + ANG_OF], nc = bas[sh * BAS_SLOTS + NCTR_OF];
+    const int e = (*sph ? 2 * l + 1 : (l + 1) * (l + 2) / 2) * nc;
+    ext.push_back(e);
+    n *= e;
+  }
+  // cintx-compat accepts dims only equal to the natural extents (compat/src/layout.rs:25-62)
+  if (dims) {
+    bool same = dims_len == (size_t)nsh;
+    for (int a = 0; same && a < nsh; ++a) same = dims[a] == ext[a];
+    if (!same) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "dims must equal the natural extents of the block");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+  }
+  *nout = n;
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintrs_query_workspace(int api, const int* dims, size_t dims_len, const int* shls, size_t shls_len, const int* atm,
+                           size_t atm_len, const int* bas, size_t bas_len, const double* env, size_t env_len,
+                           const CINTOpt* opt, CintxWorkspaceQuery* query_out) {
+  clear_error();
+  (void)opt;
+  if (!query_out) {
+    set_error(CINTX_STATUS_NULL_POINTER, "query_out must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  int family;
+  bool sph;
+  long long nout;
+  int rc = dispatch_prepare(api, dims, dims_len, shls, shls_len, atm, atm_len, bas, bas_len, env, env_len, &family,
+                            &sph, &nout);
+  if (rc) return rc;
+  query_out->bytes = 0;  // device working memory is held by the library, not the caller's cache
+  query_out->alignment = 8;
+  query_out->required_bytes = (size_t)nout * sizeof(double);
+  query_out->chunk_count = 1;
+  query_out->work_units = 1;
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintrs_eval(int api, double* out, size_t out_len, const int* dims, size_t dims_len, const int* shls,
+                size_t shls_len, const int* atm, size_t atm_len, const int* bas, size_t bas_len, const double* env,
+                size_t env_len, const CINTOpt* opt, double* cache, size_t cache_len, CintxEvalSummary* summary_out) {
+  clear_error();
+  if (!summary_out) {
+    set_error(CINTX_STATUS_NULL_POINTER, "summary_out must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if ((!out && out_len > 0) || (!cache && cache_len > 0)) {
+    set_error(CINTX_STATUS_NULL_POINTER, "out or cache is NULL with a nonzero length");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (out && cache && out == cache) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "`out` and `cache` pointers must not alias");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  int family;
+  bool sph;
+  long long nout;
+  int rc = dispatch_prepare(api, dims, dims_len, shls, shls_len, atm, atm_len, bas, bas_len, env, env_len, &family,
+                            &sph, &nout);
+  if (rc) return rc;
+  summary_out->not0 = 0;
+  summary_out->bytes_written = 0;
+  summary_out->workspace_bytes = 0;
+  if (!out) return CINTX_STATUS_SUCCESS;  // a workspace-only call
+  if ((long long)out_len < nout) {
+    set_error(CINTX_STATUS_BUFFER_TOO_SMALL, "out holds " + std::to_string(out_len) + " doubles, the block needs " +
+                                                  std::to_string(nout));
+    return CINTX_STATUS_BUFFER_TOO_SMALL;
+  }
+  const int natm = (int)(atm_len / ATM_SLOTS), nbas = (int)(bas_len / BAS_SLOTS);
+  const int r = eval_call(family, sph, out, nullptr, const_cast<int*>(shls), const_cast<int*>(atm), natm,
+                          const_cast<int*>(bas), nbas, const_cast<double*>(env), const_cast<CINTOpt*>(opt));
+  if (g_err.code) return g_err.code;
+  summary_out->not0 = r;
+  summary_out->bytes_written = (size_t)nout * sizeof(double);
+  return CINTX_STATUS_SUCCESS;
+}
+
 void int2e_optimizer(CINTOpt** opt, int* atm, int natm, int* bas, int nbas, double* env) {
   make_optimizer(opt, atm, natm, bas, nbas, env);
 }

@@ -123,6 +123,38 @@ CINTX_API int cintx_plan_shells(CintxPlan **plan, CINTOpt *opt, int family, cons
 CINTX_API int cintx_plan_int2e_screened(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
                               int64_t max_chunk_doubles);
 
+/* ---- cintx-capi id dispatch (crates/cintx-capi/src/shim.rs:312-453) --------------------- */
+
+/* Workspace and result descriptors of cintx-capi (shim.rs:52-68), field for field. */
+typedef struct {
+  size_t bytes;           /* caller cache bytes needed (0: the library holds its device memory) */
+  size_t alignment;
+  size_t required_bytes;  /* bytes of the output block */
+  size_t chunk_count;
+  size_t work_units;
+} CintxWorkspaceQuery;
+typedef struct {
+  int not0;               /* libcint's return value: 1 if any primitive survived screening */
+  size_t bytes_written;
+  size_t workspace_bytes;
+} CintxEvalSummary;
+
+/* cintrs_eval / cintrs_query_workspace for the api ids 9 int2e_cart, 10 int2e_sph, 12 int2c2e_cart,
+ * 13 int2c2e_sph (CintxRawApi, shim.rs:8-50; other ids return CINTX_STATUS_UNSUPPORTED_API).
+ * natm = atm_len / 6 and nbas = bas_len / 8; every env slot the basis references must lie below
+ * env_len; dims, when given, must equal the block's natural extents (cintx-compat layout.rs);
+ * out == NULL (out_len 0) is a workspace-only call; out and cache must not alias; opt is NULL or
+ * an optimizer of this library.  Statuses and the thread-local last error follow cintx-capi's
+ * errors.rs:9-21. */
+CINTX_API int cintrs_query_workspace(int api, const int *dims, size_t dims_len, const int *shls, size_t shls_len,
+                                     const int *atm, size_t atm_len, const int *bas, size_t bas_len,
+                                     const double *env, size_t env_len, const CINTOpt *opt,
+                                     CintxWorkspaceQuery *query_out);
+CINTX_API int cintrs_eval(int api, double *out, size_t out_len, const int *dims, size_t dims_len, const int *shls,
+                          size_t shls_len, const int *atm, size_t atm_len, const int *bas, size_t bas_len,
+                          const double *env, size_t env_len, const CINTOpt *opt, double *cache, size_t cache_len,
+                          CintxEvalSummary *summary_out);
+
 /* Device bytes held by an optimizer handle (pair and primitive-pair tables). */
 CINTX_API int64_t cintx_opt_device_bytes(CINTOpt *opt);
 

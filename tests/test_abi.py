@@ -64,3 +64,63 @@ def test_error_state_without_device():
     n = _lib.lib.int2e_sph(None, None, ok.ctypes.data_as(_lib._ip), mol.atm.ctypes.data_as(_lib._ip), mol.natm,
                            mol.bas.ctypes.data_as(_lib._ip), mol.nbas, mol.env.ctypes.data_as(_lib._dp), None, None)
     assert n > 0
+
+
+class _Summary(__import__("ctypes").Structure):
+    import ctypes as _c
+    _fields_ = [("not0", _c.c_int), ("bytes_written", _c.c_size_t), ("workspace_bytes", _c.c_size_t)]
+
+
+class _Query(__import__("ctypes").Structure):
+    import ctypes as _c
+    _fields_ = [("bytes", _c.c_size_t), ("alignment", _c.c_size_t), ("required_bytes", _c.c_size_t),
+                ("chunk_count", _c.c_size_t), ("work_units", _c.c_size_t)]
+
+
+def _dispatch_args(mol, shls):
+    import ctypes
+    import numpy as np
+    a = np.ascontiguousarray(mol.atm, dtype=np.int32).ravel()
+    b = np.ascontiguousarray(mol.bas, dtype=np.int32).ravel()
+    e = np.ascontiguousarray(mol.env, dtype=np.float64)
+    s = np.ascontiguousarray(shls, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    return (s, a, b, e), (s.ctypes.data_as(ip), s.size, a.ctypes.data_as(ip), a.size, b.ctypes.data_as(ip), b.size,
+                          e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), e.size)
+
+
+def test_cintrs_dispatch_statuses_without_device_work():
+    """cintx-capi id dispatch: statuses of the argument checks and the workspace query (host only)."""
+    import ctypes
+    import numpy as np
+    from cintx_b200 import _lib
+    from cintx_b200 import molecules as M
+    L = _lib.lib
+    mol = M.water_like()
+    keep, (s, ns, a, na, b, nb, e, ne) = _dispatch_args(mol, [5, 0, 4, 3])
+    q = _Query()
+    f = L.cintrs_query_workspace
+    f.restype = ctypes.c_int
+    rc = f(10, None, 0, s, ns, a, na, b, nb, e, ne, None, ctypes.byref(q))
+    assert rc == 0 and q.required_bytes == 8 * 5 * 1 * 3 * 3 and q.chunk_count == 1
+    assert f(11, None, 0, s, ns, a, na, b, nb, e, ne, None, ctypes.byref(q)) == 2  # spinor: unsupported
+    assert f(10, None, 0, s, ns, a, na, b, nb, e, ne, None, None) == 8
+    ev = L.cintrs_eval
+    ev.restype = ctypes.c_int
+    summ = _Summary()
+    out = np.zeros(45)
+    dp = ctypes.POINTER(ctypes.c_double)
+    args = (s, ns, a, na, b, nb, e, ne, None)
+    assert ev(10, None, 0, None, 0, *args, None, 0, ctypes.byref(summ)) == 0  # workspace-only call
+    assert summ.bytes_written == 0
+    assert ev(10, None, 5, None, 0, *args, None, 0, ctypes.byref(summ)) == 8  # NULL out with a length
+    assert ev(10, out.ctypes.data_as(dp), 45, None, 0, *args, out.ctypes.data_as(dp), 45, ctypes.byref(summ)) == 1
+    assert ev(10, out.ctypes.data_as(dp), 44, None, 0, *args, None, 0, ctypes.byref(summ)) == 4  # too small
+    bad_dims = np.array([5, 1, 3, 4], dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    assert ev(10, out.ctypes.data_as(dp), 45, bad_dims.ctypes.data_as(ip), 4, *args, None, 0,
+              ctypes.byref(summ)) == 1
+    assert ev(10, out.ctypes.data_as(dp), 45, None, 0, s, ns, a, na, b, nb, e, 3, None, None, 0,
+              ctypes.byref(summ)) == 1  # env shorter than the basis needs
+    code, msg = _lib.last_error()
+    assert code == 1 and "env" in msg

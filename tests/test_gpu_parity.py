@@ -315,3 +315,23 @@ def test_unsupported_inputs_report_errors(cx):
     with pytest.raises(cx.CintxError) as e:
         cx.int2e_sph((0, 0, 0, 0), mol.atm, mol.bas, env)
     assert e.value.code == 2
+
+
+def test_cintrs_eval_matches_libcint_signature(cx):
+    """cintx-capi's id dispatch returns the same blocks and not0 as int2e_sph / int2c2e_cart."""
+    import ctypes
+    from test_abi import _Summary, _dispatch_args
+    mol = M.water_like()
+    dp = ctypes.POINTER(ctypes.c_double)
+    for api, shls, fn in [(10, [5, 0, 4, 3], lambda t: cx.int2e_sph(t, mol.atm, mol.bas, mol.env)),
+                          (9, [1, 2, 3, 4], lambda t: cx.int2e_cart(t, mol.atm, mol.bas, mol.env)),
+                          (12, [5, 3], lambda t: cx.int2c2e_cart(t, mol.atm, mol.bas, mol.env)),
+                          (13, [5, 3], lambda t: cx.int2c2e_sph(t, mol.atm, mol.bas, mol.env))]:
+        ref, ret = fn(shls)
+        keep, args = _dispatch_args(mol, shls)
+        out = np.full(ref.size, np.nan)
+        summ = _Summary()
+        rc = cx.lib.cintrs_eval(api, out.ctypes.data_as(dp), out.size, None, 0, *args, None, None, 0,
+                                ctypes.byref(summ))
+        assert rc == 0 and summ.not0 == ret and summ.bytes_written == 8 * ref.size
+        assert np.array_equal(out, ref)
