@@ -82,6 +82,7 @@ def parse():
     ap.add_argument("--error-chunks", type=int, default=4)
     ap.add_argument("--fp32-budget", type=float, default=FP32_BUDGET)
     ap.add_argument("--no-autotune", action="store_true", help="tuned form without the launch-shape autotuner")
+    ap.add_argument("--no-jk", action="store_true", help="skip the direct J/K build timing")
     ap.add_argument("--e2e-chunk-doubles", type=int, default=1 << 24,
                     help="chunk size of the end-to-end plan (copies of one chunk overlap the next chunk's kernels)")
     ap.add_argument("--prim-budget", type=float, default=PRIM_BUDGET)
@@ -477,6 +478,43 @@ def class_profile(torch, plan, mine, ring, stream):
     return per_class
 
 
+def jk_timing(cx, torch, plan, mol, stream, reps):
+    """Direct Coulomb + exchange build over the sweep (cintx_plan_jk): device time per build (CUDA
+    events, after one warm-up) and end to end with the density copied in and J, K copied out."""
+    nao = int(mol.ao_loc()[-1])
+    rng = np.random.default_rng(11)
+    dh = rng.normal(size=(nao, nao))
+    dh = torch.tensor(dh + dh.T).pin_memory()
+    d = torch.empty((nao, nao), dtype=torch.float64, device="cuda")
+    vj = torch.empty_like(d)
+    vk = torch.empty_like(d)
+    hj = torch.empty((nao, nao), dtype=torch.float64).pin_memory()
+    hk = torch.empty_like(hj).pin_memory()
+    d.copy_(dh, non_blocking=True)
+    plan.jk(d.data_ptr(), nao, vj.data_ptr(), vk.data_ptr(), stream=stream.cuda_stream)  # warm-up
+    stream.synchronize()
+    ms, e2e = [], []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        d.copy_(dh, non_blocking=True)
+        e0.record(stream)
+        plan.jk(d.data_ptr(), nao, vj.data_ptr(), vk.data_ptr(), stream=stream.cuda_stream)
+        e1.record(stream)
+        hj.copy_(vj, non_blocking=True)
+        hk.copy_(vk, non_blocking=True)
+        stream.synchronize()
+        e2e.append(time.perf_counter() - t0)
+        ms.append(e0.elapsed_time(e1))
+    st = plan.stats
+    t = statistics.mean(ms)
+    return {"ms_per_build": t, "nao": nao, "integrals_contracted_per_s": st.nintegrals / (t * 1e-3),
+            "e2e_ms_per_build": statistics.mean(e2e) * 1e3,
+            "e2e_bytes": {"h2d": nao * nao * 8, "d2h": 2 * nao * nao * 8},
+            "what": "J = (pq|rs) D_rs and K = (pq|rs) D_qs over the same quartet set, each chunk contracted "
+                    "on the device right after its kernels (8-fold symmetry); integrals never leave the GPU"}
+
+
 def tuned_error(cx, torch, opt, plan, ring, stream, max_chunks):
     """Max and RMS absolute difference between the mixed plan and an FP64 evaluation of the same
     quartets (explicit FP64 plan over each checked chunk's quartet list)."""
@@ -564,6 +602,9 @@ def our_arm(args):
     err = None
     if tuned and rank == 0 and not args.no_error:
         err = tuned_error(cx, torch, opt, plan, main_run["ring"], stream, args.error_chunks)
+    jk = None
+    if rank == 0 and world == 1 and not args.no_jk:
+        jk = jk_timing(cx, torch, plan, mol, stream, min(args.steps, 5))
     if rank != 0:
         if world > 1:
             dist.barrier()
@@ -611,6 +652,8 @@ def our_arm(args):
         line["tuned_over_plain"] = value / plain["value"]
     if err is not None:
         line["error_vs_fp64"] = err
+    if jk is not None:
+        line["jk_build"] = jk
 
     # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1):
     # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory

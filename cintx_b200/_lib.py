@@ -83,6 +83,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute_host.restype = _i
     L.cintx_plan_execute_host_ring.argtypes = [_vp, _dp, _i64, ctypes.c_void_p, ctypes.c_void_p]
     L.cintx_plan_execute_host_ring.restype = _i
+    L.cintx_plan_jk.argtypes = [_vp, _vp, _i, _vp, _vp, _vp]
+    L.cintx_plan_jk.restype = _i
     L.cintx_plan_autotune.argtypes = [_vp, _i64, ctypes.c_void_p, ctypes.c_void_p, _i]
     L.cintx_plan_autotune.restype = _i
     L.cintx_plan_use_tuned_shapes.argtypes = [_vp]
@@ -359,6 +361,12 @@ class Plan:
         on its largest segment in the plan).  Synchronous; a captured graph is released and must
         be built again."""
         _check(lib.cintx_plan_autotune(self.handle, chunk, ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream), reps))
+
+    def jk(self, dm_ptr: int, nao: int, vj_ptr: int = 0, vk_ptr: int = 0, stream: int = 0):
+        """Coulomb (vj) and exchange (vk) matrices for the symmetric density at dm_ptr (device
+        pointers, row-major nao x nao; 0 skips an output).  Asynchronous on stream."""
+        _check(lib.cintx_plan_jk(self.handle, ctypes.c_void_p(dm_ptr), int(nao), ctypes.c_void_p(vj_ptr or None),
+                                 ctypes.c_void_p(vk_ptr or None), ctypes.c_void_p(stream)))
 
     def use_tuned_shapes(self) -> int:
         """Reuse the launch shapes autotuned earlier in this process; returns segments changed."""

@@ -31,6 +31,9 @@ cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPai
                           const long long* pbase, double* xout, cudaStream_t stream);
 cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, const double* out, const long long* len,
                                      double* q, cudaStream_t stream);
+cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream);
+cudaError_t launch_symmetrize(const double* X, double* M, int n, cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -113,6 +116,11 @@ struct CintxPlan {
   // quartet, and per record its base (doubles) in d_rootbuf
   double* d_rootbuf = nullptr;
   long long* d_rootbase = nullptr;
+  // J/K builds (cintx_plan_jk): shells of each regular pair, AO offsets, accumulators, chunk ring
+  int2* d_psh = nullptr;
+  int* d_aoloc = nullptr;
+  double* d_jkacc = nullptr;
+  long long jk_cap = 0;
   cudaEvent_t ev_done[2] = {nullptr, nullptr};
   cudaEvent_t ev_free[2] = {nullptr, nullptr};
 };
@@ -699,6 +707,78 @@ int cintx_plan_use_learned_roots(CintxPlan* p, const float* params, int64_t* nfa
   }
   if (nfallback) *nfallback = fb;
   if (npoints) *npoints = total;
+  return CINTX_STATUS_SUCCESS;
+}
+
+int cintx_plan_jk(CintxPlan* p, const double* dm, int nao, double* vj, double* vk, void* stream_) {
+  clear_error();
+  if (!p || !dm || (!vj && !vk)) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan, dm and one of vj / vk must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (p->tiles.empty() || p->family != CINTX_INT2E) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "J/K builds run over an int2e unique-quartet sweep (cintx_plan_int2e_screened)");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  const Opt* o = p->opt;
+  const Basis& B = o->basis;
+  std::vector<int> aoloc(B.nbas + 1, 0);
+  for (int sh = 0; sh < B.nbas; ++sh) aoloc[sh + 1] = aoloc[sh] + nsph_or_cart(B.sh[sh].l, p->sph);
+  if (nao != aoloc[B.nbas]) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "nao is " + std::to_string(nao) + ", the basis has " +
+                                              std::to_string(aoloc[B.nbas]) + " functions");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  cudaStream_t stream = (cudaStream_t)stream_;
+  long long slot = 1;
+  for (const Chunk& c : p->chunks) slot = std::max(slot, c.out_size);
+  const long long acc = 2LL * nao * nao;
+  bool ok = true;
+  if (!p->d_psh) {
+    std::vector<int2> psh(o->npairs);
+    for (int id = 0; id < o->npairs; ++id) psh[id] = make_int2(B.vshell[o->pair_a[id]], B.vshell[o->pair_b[id]]);
+    ok = cudaMalloc(&p->d_psh, sizeof(int2) * std::max(o->npairs, 1)) == cudaSuccess &&
+         cudaMalloc(&p->d_aoloc, sizeof(int) * aoloc.size()) == cudaSuccess;
+    if (ok) {
+      cudaMemcpy(p->d_psh, psh.data(), sizeof(int2) * psh.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(p->d_aoloc, aoloc.data(), sizeof(int) * aoloc.size(), cudaMemcpyHostToDevice);
+    }
+  }
+  if (ok && acc > p->jk_cap) {
+    if (p->d_jkacc) cudaFree(p->d_jkacc);
+    ok = cudaMalloc(&p->d_jkacc, sizeof(double) * acc) == cudaSuccess;
+    p->jk_cap = ok ? acc : 0;
+    if (!ok) p->d_jkacc = nullptr;
+  }
+  if (ok && slot > p->stage_cap) {
+    if (p->d_stage) cudaFree(p->d_stage);
+    ok = cudaMalloc(&p->d_stage, sizeof(double) * slot) == cudaSuccess;
+    p->stage_cap = ok ? slot : 0;
+    if (!ok) p->d_stage = nullptr;
+  }
+  if (!ok) {
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the J/K build failed");
+    return CINTX_STATUS_ALLOCATION_FAILED;
+  }
+  double* A = vj ? p->d_jkacc : nullptr;
+  double* Bk = vk ? p->d_jkacc + (size_t)nao * nao : nullptr;
+  cudaMemsetAsync(p->d_jkacc, 0, sizeof(double) * acc, stream);
+  // each chunk: the sweep's kernels into the ring, then its contraction (same stream, so the
+  // next chunk's record generation waits for the contraction to have read the records)
+  for (int64_t c = 0; c < (int64_t)p->chunks.size(); ++c) {
+    int rc = cintx_plan_execute(p, c, p->d_stage, stream);
+    if (rc) return rc;
+    if (launch_jk_contract(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc, p->d_stage, dm, nao, A, Bk, stream) !=
+        cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "J/K contraction launch failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+  }
+  if ((vj && launch_symmetrize(A, vj, nao, stream) != cudaSuccess) ||
+      (vk && launch_symmetrize(Bk, vk, nao, stream) != cudaSuccess)) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "J/K symmetrisation launch failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
   return CINTX_STATUS_SUCCESS;
 }
 

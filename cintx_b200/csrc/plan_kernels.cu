@@ -112,6 +112,87 @@ __global__ void block_absmax_sqrt_kernel(const QuartetRec* __restrict__ recs, lo
   }
 }
 
+// Coulomb/exchange contraction of one chunk of a unique-quartet sweep (a >= b, c >= d, ab >= cd):
+// one warp per quartet block v[i + ni*(j + nj*(k + nk*l))] (shells a, b, c, d), with the 8-fold
+// permutational symmetry of real integrals and a symmetric density D (row-major nao x nao):
+//   A[i,j] += 2 s sum_kl v D[k,l],  A[k,l] += 2 s sum_ij v D[i,j]          (J = A + A^T)
+//   B[i,k] += s sum_jl v D[j,l],  B[j,k] += s sum_il v D[i,l],
+//   B[i,l] += s sum_jk v D[j,k],  B[j,l] += s sum_ik v D[i,k]               (K = B + B^T)
+// with s = 1/2 for each of a == b, c == d, (ab) == (cd) (those blocks hold every element twice).
+// Each (row, column) pair of a block reduces its sum first and adds it with one atomic.
+__global__ void jk_contract_kernel(const QuartetRec* __restrict__ recs, long long nrec, const int2* __restrict__ psh,
+                                   const int* __restrict__ aoloc, const double* __restrict__ out,
+                                   const double* __restrict__ dm, int nao, double* __restrict__ A,
+                                   double* __restrict__ B) {
+  const int lane = threadIdx.x & 31;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nrec;
+       r += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const QuartetRec rec = recs[r];
+    const int2 ab = psh[rec.pij], cd = psh[rec.pkl];
+    const int i0 = aoloc[ab.x], j0 = aoloc[ab.y], k0 = aoloc[cd.x], l0 = aoloc[cd.y];
+    const int ni = aoloc[ab.x + 1] - i0, nj = aoloc[ab.y + 1] - j0;
+    const int nk = aoloc[cd.x + 1] - k0, nl = aoloc[cd.y + 1] - l0;
+    const double s = (ab.x == ab.y ? 0.5 : 1.0) * (cd.x == cd.y ? 0.5 : 1.0) * (rec.pij == rec.pkl ? 0.5 : 1.0);
+    const double* v = out + rec.out;
+    const int sj = ni, sk = ni * nj, sl = ni * nj * nk;
+    if (A) {
+      for (int e = lane; e < ni * nj; e += 32) {
+        const int i = e % ni, j = e / ni;
+        double t = 0.0;
+        for (int l = 0; l < nl; ++l)
+          for (int k = 0; k < nk; ++k) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(k0 + k) * nao + l0 + l];
+        atomicAdd(A + (size_t)(i0 + i) * nao + j0 + j, 2.0 * s * t);
+      }
+      for (int e = lane; e < nk * nl; e += 32) {
+        const int k = e % nk, l = e / nk;
+        double t = 0.0;
+        for (int j = 0; j < nj; ++j)
+          for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + j0 + j];
+        atomicAdd(A + (size_t)(k0 + k) * nao + l0 + l, 2.0 * s * t);
+      }
+    }
+    if (B) {
+      for (int e = lane; e < ni * nk; e += 32) {  // B[i,k] += s sum_jl v D[j,l]
+        const int i = e % ni, k = e / ni;
+        double t = 0.0;
+        for (int l = 0; l < nl; ++l)
+          for (int j = 0; j < nj; ++j) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(j0 + j) * nao + l0 + l];
+        atomicAdd(B + (size_t)(i0 + i) * nao + k0 + k, s * t);
+      }
+      for (int e = lane; e < nj * nk; e += 32) {  // B[j,k] += s sum_il v D[i,l]
+        const int j = e % nj, k = e / nj;
+        double t = 0.0;
+        for (int l = 0; l < nl; ++l)
+          for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + l0 + l];
+        atomicAdd(B + (size_t)(j0 + j) * nao + k0 + k, s * t);
+      }
+      for (int e = lane; e < ni * nl; e += 32) {  // B[i,l] += s sum_jk v D[j,k]
+        const int i = e % ni, l = e / ni;
+        double t = 0.0;
+        for (int k = 0; k < nk; ++k)
+          for (int j = 0; j < nj; ++j) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(j0 + j) * nao + k0 + k];
+        atomicAdd(B + (size_t)(i0 + i) * nao + l0 + l, s * t);
+      }
+      for (int e = lane; e < nj * nl; e += 32) {  // B[j,l] += s sum_ik v D[i,k]
+        const int j = e % nj, l = e / nj;
+        double t = 0.0;
+        for (int k = 0; k < nk; ++k)
+          for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + k0 + k];
+        atomicAdd(B + (size_t)(j0 + j) * nao + l0 + l, s * t);
+      }
+    }
+  }
+}
+
+// M[p,q] = X[p,q] + X[q,p] (n x n), for J = A + A^T and K = B + B^T.
+__global__ void symmetrize_kernel(const double* __restrict__ X, double* __restrict__ M, int n) {
+  const long long total = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(e / n), q = (int)(e % n);
+    M[e] = X[e] + X[(size_t)q * n + p];
+  }
+}
+
 namespace cintx {
 cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPair* pairs, const PrimPair* prims,
                           const long long* pbase, double* xout, cudaStream_t stream) {
@@ -128,6 +209,23 @@ cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, con
   long long blocks = (nrec * 32 + 255) / 256;
   if (blocks > 65535) blocks = 65535;
   block_absmax_sqrt_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, out, len, q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec * 32 + 255) / 256;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  jk_contract_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, dm, nao, A, B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_symmetrize(const double* X, double* M, int n, cudaStream_t stream) {
+  const long long total = (long long)n * n;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  if (total > 0) symmetrize_kernel<<<(unsigned)blocks, 256, 0, stream>>>(X, M, n);
   return cudaGetLastError();
 }
 

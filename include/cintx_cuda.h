@@ -192,6 +192,16 @@ CINTX_API int cintx_optimizer_pair_shells(CINTOpt **opt, const int *atm, int nat
 CINTX_API int cintx_plan_int3c2e_screened(CintxPlan **plan, CINTOpt *opt, double cutoff, int sph,
                                           int64_t max_chunk_doubles, int norb);
 
+/* Coulomb and exchange matrices of a unique-quartet int2e sweep (cintx_plan_int2e_screened or
+ * cintx_plan_int2e_screened_mixed) for a symmetric density dm (device, row-major nao x nao in this
+ * plan's representation, AOs ordered by shell): vj[p,q] = sum_rs (pq|rs) dm[r,s] and
+ * vk[p,r] = sum_qs (pq|rs) dm[q,s] (device, nao x nao; either may be NULL), without writing the
+ * integrals anywhere but a device chunk ring.  Each chunk's blocks are contracted right after its
+ * kernels with the 8-fold permutational symmetry.  Asynchronous on stream; the plan's device
+ * buffers are reused, so calls on one plan must not overlap.  No counterpart in libcint (the
+ * direct-SCF consumer of int2e_sph, e.g. PySCF's vhf). */
+CINTX_API int cintx_plan_jk(CintxPlan *plan, const double *dm, int nao, double *vj, double *vk, void *stream);
+
 /* Plan statistics. */
 typedef struct {
   int64_t nquartets;        /* shell tuples in the plan */
