@@ -1265,7 +1265,9 @@ int compute_prim_schwarz(Opt* o) {
     std::vector<int> pa(n), pb(n);
     for (int i = 0; i < n; ++i) {
       pp[i] = o->h_prims[k0 + ord[i]];
-      pp[i].q = qv[ord[i]];
+      // scaled by the pair's primitive count P: q'_ab q'_cd < eps bounds a quartet's dropped
+      // primitive terms by P_ab P_cd max(q_ab q_cd) < eps whatever the quartet's primitive counts
+      pp[i].q = qv[ord[i]] * n;
       pa[i] = o->h_prim_a[k0 + ord[i]];
       pb[i] = o->h_prim_b[k0 + ord[i]];
     }
@@ -1340,25 +1342,16 @@ static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk,
       flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
     }
   }
-  // primitive screening threshold per kernel class and precision: the dropped primitive
-  // quartets of one contracted quartet sum to at most prim_budget in its spherical block
+  // primitive screening threshold per kernel class and precision: with the primitive factors
+  // scaled by their pair's primitive count (compute_prim_schwarz), the dropped primitive quartets
+  // of one contracted quartet sum to at most prim_budget / (c2s amplification) in its cartesian
+  // block, hence prim_budget in its spherical block
   std::map<std::tuple<int, int, int, int, int>, double> class_eps;
-  if (prim_budget > 0) {
-    std::map<std::tuple<int, int, int, int, int>, double> maxprod;
+  if (prim_budget > 0)
     for (const Tile& t : p->tiles) {
-      int mr = 1, mc = 1;
-      for (int id : t.rows) mr = std::max(mr, o->pair_nprim[id]);
-      for (int id : t.cols) mc = std::max(mc, o->pair_nprim[id]);
-      auto key = std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32);
-      maxprod[key] = std::max(maxprod[key], (double)mr * mc);
+      const double amp = c2s_amp(t.li, p->sph) * c2s_amp(t.lj, p->sph) * c2s_amp(t.lk, p->sph) * c2s_amp(t.ll, p->sph);
+      class_eps[std::make_tuple(t.li, t.lj, t.lk, t.ll, (int)t.fp32)] = prim_budget / amp;
     }
-    for (auto& kv : maxprod) {
-      const int li = std::get<0>(kv.first), lj = std::get<1>(kv.first), lk = std::get<2>(kv.first),
-                ll = std::get<3>(kv.first);
-      const double amp = c2s_amp(li, p->sph) * c2s_amp(lj, p->sph) * c2s_amp(lk, p->sph) * c2s_amp(ll, p->sph);
-      class_eps[kv.first] = prim_budget / (kv.second * amp);
-    }
-  }
   // 3. chunks: greedy fill up to max_chunk doubles, splitting tiles at quartet boundaries
   Chunk cur;
   long long max_recs = 0;
