@@ -105,7 +105,11 @@ struct EriShape {
   // the final I values to shared memory; the others keep the 2D table in shared memory (with
   // 4+ lanes the unrolled form spills under the 128-register cap and measured slower)
   static constexpr bool REG_RECUR = S <= 2 && NIJ * NKL <= 16 && GSZ <= 36;
-  static constexpr int NTASK_CONC = S < 3 * NR ? S : 3 * NR;  // tasks running at once
+  // non-default launch shapes with at least twice as many lanes as (axis, root) tasks split each
+  // task's horizontal transfers over NPARTS lanes (the default shape keeps one lane per task)
+  static constexpr int NPARTS_RAW = (!(ACC == 24 && REGS == 128) && !REG_RECUR && S >= 6 * NR) ? S / (3 * NR) : 1;
+  static constexpr int NPARTS = NPARTS_RAW < NI ? NPARTS_RAW : NI;
+  static constexpr int NTASK_CONC = S < 3 * NR * NPARTS ? S : 3 * NR * NPARTS;  // tasks running at once
   static constexpr int SM_SCR = REG_RECUR ? 0 : NTASK_CONC * NIJ * NKL;  // per-task 2D tables
   // classes whose transform buffers do not fit on chip keep them in a per-block global scratch
   static constexpr bool GLOBAL_BUF = S > 1 && (SM_BUFA + SM_BUFB) * 8 * (S >= 128 ? 1 : 128 / S) > 200 * 1024;
@@ -196,9 +200,11 @@ __device__ __forceinline__ void vrr_hrr(R* __restrict__ dst, R g00, R c00, R c0p
 
 // Shared-memory version for the multi-lane path: the 2D table lives in gs[n*NKL + m]; the
 // horizontal transfers are unrolled over j and the (k, l) outputs, looped over i.
-template <int LI, int LJ, int LK, int LL, class R = double>
+// NPARTS > 1: this call writes only the i = part, part + NPARTS, ... rows of the transfers (the
+// other parts of the same (axis, root) task run on other lanes, each with its own 2D table).
+template <int LI, int LJ, int LK, int LL, class R = double, int NPARTS = 1>
 __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict__ gs, R g00, R c00, R c0p, R b10,
-                                             R b01, R b00, R ab, R cd) {
+                                             R b01, R b00, R ab, R cd, int part = 0) {
   constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
   constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
   {
@@ -226,7 +232,7 @@ __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict_
   cdp[0] = (R)1;
 #pragma unroll
   for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
-  for (int i = 0; i <= LI; ++i) {
+  for (int i = NPARTS > 1 ? part : 0; i <= LI; i += NPARTS) {
 #pragma unroll
     for (int j = 0; j <= LJ; ++j) {
       R T[NKL];
@@ -495,7 +501,8 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
         }
         group_sync<S>(group);
         // (axis, root) recurrences, one per lane; coefficients in FP64, recurrences in R
-        for (int task = lane; task < 3 * NR; task += S) {
+        for (int tp = lane; tp < 3 * NR * SH::NPARTS; tp += S) {
+          const int task = tp / SH::NPARTS, part = tp % SH::NPARTS;
           const int axis = task / NR, r = task % NR;
           const double t2 = s_roots[r];
           const double rt_aa = t2 * inv_aijkl;
@@ -512,9 +519,10 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
             vrr_hrr<LI, LJ, LK, LL, R>(s_g + task * GSZ, (R)g00, (R)(pa - rt_aa * akl * pq),
                                        (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab, (R)cd);
           } else {
-            vrr_hrr_smem<LI, LJ, LK, LL, R>(s_g + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL), (R)g00,
-                                            (R)(pa - rt_aa * akl * pq), (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01,
-                                            (R)b00, (R)ab, (R)cd);
+            vrr_hrr_smem<LI, LJ, LK, LL, R, SH::NPARTS>(s_g + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL),
+                                                        (R)g00, (R)(pa - rt_aa * akl * pq),
+                                                        (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab,
+                                                        (R)cd, part);
           }
         }
         group_sync<S>(group);
