@@ -83,6 +83,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute_host.restype = _i
     L.cintx_plan_execute_host_ring.argtypes = [_vp, _dp, _i64, ctypes.c_void_p, ctypes.c_void_p]
     L.cintx_plan_execute_host_ring.restype = _i
+    L.cintx_plan_execute_s8.argtypes = [_vp, _vp, _i64, _vp]
+    L.cintx_plan_execute_s8.restype = _i
     L.cintx_plan_jk.argtypes = [_vp, _vp, _i, _vp, _vp, _vp]
     L.cintx_plan_jk.restype = _i
     L.cintx_plan_autotune.argtypes = [_vp, _i64, ctypes.c_void_p, ctypes.c_void_p, _i]
@@ -367,6 +369,10 @@ class Plan:
         pointers, row-major nao x nao; 0 skips an output).  Asynchronous on stream."""
         _check(lib.cintx_plan_jk(self.handle, ctypes.c_void_p(dm_ptr), int(nao), ctypes.c_void_p(vj_ptr or None),
                                  ctypes.c_void_p(vk_ptr or None), ctypes.c_void_p(stream)))
+
+    def execute_s8(self, eri_ptr: int, length: int, stream: int = 0):
+        """The sweep as the 8-fold packed AO tensor at device pointer eri_ptr (length doubles)."""
+        _check(lib.cintx_plan_execute_s8(self.handle, ctypes.c_void_p(eri_ptr), int(length), ctypes.c_void_p(stream)))
 
     def use_tuned_shapes(self) -> int:
         """Reuse the launch shapes autotuned earlier in this process; returns segments changed."""

@@ -34,6 +34,8 @@ cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, con
 cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
                                const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream);
 cudaError_t launch_symmetrize(const double* X, double* M, int n, cudaStream_t stream);
+cudaError_t launch_scatter_s8(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                              const double* out, double* eri, cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -710,6 +712,67 @@ int cintx_plan_use_learned_roots(CintxPlan* p, const float* params, int64_t* nfa
   return CINTX_STATUS_SUCCESS;
 }
 
+// Device copies of each regular pair's shells and of the AO offsets (cached in the plan).
+static bool ao_maps(CintxPlan* p, const std::vector<int>& aoloc) {
+  if (p->d_psh) return true;
+  const Opt* o = p->opt;
+  const Basis& B = o->basis;
+  std::vector<int2> psh(o->npairs);
+  for (int id = 0; id < o->npairs; ++id) psh[id] = make_int2(B.vshell[o->pair_a[id]], B.vshell[o->pair_b[id]]);
+  bool ok = cudaMalloc(&p->d_psh, sizeof(int2) * std::max(o->npairs, 1)) == cudaSuccess &&
+            cudaMalloc(&p->d_aoloc, sizeof(int) * aoloc.size()) == cudaSuccess;
+  if (ok) {
+    cudaMemcpy(p->d_psh, psh.data(), sizeof(int2) * psh.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(p->d_aoloc, aoloc.data(), sizeof(int) * aoloc.size(), cudaMemcpyHostToDevice);
+  }
+  return ok;
+}
+
+int cintx_plan_execute_s8(CintxPlan* p, double* eri, int64_t len, void* stream_) {
+  clear_error();
+  if (!p || !eri) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan and eri must not be NULL");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  if (p->tiles.empty() || p->family != CINTX_INT2E) {
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "the packed AO tensor is written from an int2e unique-quartet sweep");
+    return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  const Basis& B = p->opt->basis;
+  std::vector<int> aoloc(B.nbas + 1, 0);
+  for (int sh = 0; sh < B.nbas; ++sh) aoloc[sh + 1] = aoloc[sh] + nsph_or_cart(B.sh[sh].l, p->sph);
+  const long long nao = aoloc[B.nbas], npair = nao * (nao + 1) / 2, need = npair * (npair + 1) / 2;
+  if (len < need) {
+    set_error(CINTX_STATUS_BUFFER_TOO_SMALL, "the packed tensor of " + std::to_string(nao) + " functions needs " +
+                                                 std::to_string(need) + " doubles");
+    return CINTX_STATUS_BUFFER_TOO_SMALL;
+  }
+  cudaStream_t stream = (cudaStream_t)stream_;
+  long long slot = 1;
+  for (const Chunk& c : p->chunks) slot = std::max(slot, c.out_size);
+  bool ok = ao_maps(p, aoloc);
+  if (ok && slot > p->stage_cap) {
+    if (p->d_stage) cudaFree(p->d_stage);
+    ok = cudaMalloc(&p->d_stage, sizeof(double) * slot) == cudaSuccess;
+    p->stage_cap = ok ? slot : 0;
+    if (!ok) p->d_stage = nullptr;
+  }
+  if (!ok) {
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the packed tensor failed");
+    return CINTX_STATUS_ALLOCATION_FAILED;
+  }
+  cudaMemsetAsync(eri, 0, sizeof(double) * need, stream);  // quartets below the cutoff stay 0
+  for (int64_t c = 0; c < (int64_t)p->chunks.size(); ++c) {
+    int rc = cintx_plan_execute(p, c, p->d_stage, stream);
+    if (rc) return rc;
+    if (launch_scatter_s8(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc, p->d_stage, eri, stream) != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "scatter launch failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
 int cintx_plan_jk(CintxPlan* p, const double* dm, int nao, double* vj, double* vk, void* stream_) {
   clear_error();
   if (!p || !dm || (!vj && !vk)) {
@@ -733,17 +796,7 @@ int cintx_plan_jk(CintxPlan* p, const double* dm, int nao, double* vj, double* v
   long long slot = 1;
   for (const Chunk& c : p->chunks) slot = std::max(slot, c.out_size);
   const long long acc = 2LL * nao * nao;
-  bool ok = true;
-  if (!p->d_psh) {
-    std::vector<int2> psh(o->npairs);
-    for (int id = 0; id < o->npairs; ++id) psh[id] = make_int2(B.vshell[o->pair_a[id]], B.vshell[o->pair_b[id]]);
-    ok = cudaMalloc(&p->d_psh, sizeof(int2) * std::max(o->npairs, 1)) == cudaSuccess &&
-         cudaMalloc(&p->d_aoloc, sizeof(int) * aoloc.size()) == cudaSuccess;
-    if (ok) {
-      cudaMemcpy(p->d_psh, psh.data(), sizeof(int2) * psh.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(p->d_aoloc, aoloc.data(), sizeof(int) * aoloc.size(), cudaMemcpyHostToDevice);
-    }
-  }
+  bool ok = ao_maps(p, aoloc);
   if (ok && acc > p->jk_cap) {
     if (p->d_jkacc) cudaFree(p->d_jkacc);
     ok = cudaMalloc(&p->d_jkacc, sizeof(double) * acc) == cudaSuccess;

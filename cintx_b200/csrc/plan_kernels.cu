@@ -184,6 +184,32 @@ __global__ void jk_contract_kernel(const QuartetRec* __restrict__ recs, long lon
   }
 }
 
+// Scatters one chunk of a unique-quartet sweep into the 8-fold packed AO tensor
+// eri[pq*(pq+1)/2 + rs] (pq = p*(p+1)/2 + q for p >= q, pq >= rs), one warp per quartet block.
+// Elements a block holds twice (diagonal shell pairs) map to the same slot and carry equal values.
+__global__ void scatter_s8_kernel(const QuartetRec* __restrict__ recs, long long nrec, const int2* __restrict__ psh,
+                                  const int* __restrict__ aoloc, const double* __restrict__ out,
+                                  double* __restrict__ eri) {
+  const int lane = threadIdx.x & 31;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nrec;
+       r += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const QuartetRec rec = recs[r];
+    const int2 ab = psh[rec.pij], cd = psh[rec.pkl];
+    const int i0 = aoloc[ab.x], j0 = aoloc[ab.y], k0 = aoloc[cd.x], l0 = aoloc[cd.y];
+    const int ni = aoloc[ab.x + 1] - i0, nj = aoloc[ab.y + 1] - j0;
+    const int nk = aoloc[cd.x + 1] - k0, nl = aoloc[cd.y + 1] - l0;
+    const int n = ni * nj * nk * nl;
+    const double* v = out + rec.out;
+    for (int e = lane; e < n; e += 32) {
+      const int i = e % ni, j = (e / ni) % nj, k = (e / (ni * nj)) % nk, l = e / (ni * nj * nk);
+      const long long p = i0 + i, q = j0 + j, u = k0 + k, w = l0 + l;
+      const long long pq = p >= q ? p * (p + 1) / 2 + q : q * (q + 1) / 2 + p;
+      const long long uw = u >= w ? u * (u + 1) / 2 + w : w * (w + 1) / 2 + u;
+      eri[pq >= uw ? pq * (pq + 1) / 2 + uw : uw * (uw + 1) / 2 + pq] = v[e];
+    }
+  }
+}
+
 // M[p,q] = X[p,q] + X[q,p] (n x n), for J = A + A^T and K = B + B^T.
 __global__ void symmetrize_kernel(const double* __restrict__ X, double* __restrict__ M, int n) {
   const long long total = (long long)n * n;
@@ -218,6 +244,15 @@ cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int
   long long blocks = (nrec * 32 + 255) / 256;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   jk_contract_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, dm, nao, A, B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_s8(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                              const double* out, double* eri, cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec * 32 + 255) / 256;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  scatter_s8_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, eri);
   return cudaGetLastError();
 }
 

@@ -201,6 +201,11 @@ CINTX_API int cintx_plan_int3c2e_screened(CintxPlan **plan, CINTOpt *opt, double
  * buffers are reused, so calls on one plan must not overlap.  No counterpart in libcint (the
  * direct-SCF consumer of int2e_sph, e.g. PySCF's vhf). */
 CINTX_API int cintx_plan_jk(CintxPlan *plan, const double *dm, int nao, double *vj, double *vk, void *stream);
+/* The whole sweep as the 8-fold packed AO tensor (PySCF ao2mo's "s8" layout): eri[pq*(pq+1)/2 + rs]
+ * with pq = p*(p+1)/2 + q (p >= q, AOs ordered by shell in this plan's representation) and
+ * pq >= rs; len >= npair*(npair+1)/2 doubles of device memory, npair = nao*(nao+1)/2.  Quartets
+ * below the plan's cutoff are 0.  Asynchronous on stream. */
+CINTX_API int cintx_plan_execute_s8(CintxPlan *plan, double *eri, int64_t len, void *stream);
 
 /* Plan statistics. */
 typedef struct {

@@ -65,3 +65,32 @@ def test_jk_matches_dense_eri(cx, name, sph):
         with pytest.raises(cx.CintxError):
             plan.jk(d.data_ptr(), n + 1, vj2.data_ptr(), 0, stream=s.cuda_stream)
         plan.close()
+
+
+@pytest.mark.parametrize("name", ["water3", "jk4"])
+def test_s8_packed_tensor_matches_dense_eri(cx, name):
+    """cintx_plan_execute_s8: every canonical slot (p >= q, r >= s, pq >= rs) of the packed AO
+    tensor against the dense oracle tensor (rtol 1e-9: the oracle evaluates each permutation of a
+    quartet independently, and those differ by up to ~1e-10 relative)."""
+    import torch
+    from oracle import Restatement
+    orc = Restatement()
+    mol = M.water_like() if name == "water3" else M.random_molecule("jk4", 9, 4, 5.0, with_f=True)
+    eri, n = _dense_eri(orc, mol, True)
+    npair = n * (n + 1) // 2
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-14, sph=True, max_chunk_doubles=1 << 12)
+        buf = torch.full((npair * (npair + 1) // 2,), float("nan"), dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream()
+        plan.execute_s8(buf.data_ptr(), buf.numel(), stream=s.cuda_stream)
+        s.synchronize()
+        got = buf.cpu().numpy()
+        with pytest.raises(cx.CintxError):
+            plan.execute_s8(buf.data_ptr(), buf.numel() - 1, stream=s.cuda_stream)
+        plan.close()
+    p, q = np.tril_indices(n)
+    ref = eri[p[:, None], q[:, None], p[None, :], q[None, :]]  # [pq, rs]
+    ii, jj = np.tril_indices(npair)
+    want = ref[ii, jj]
+    assert np.isfinite(got).all()
+    assert np.all(np.abs(got - want) <= 1e-11 + 1e-9 * np.abs(want)), np.abs(got - want).max()
