@@ -32,7 +32,8 @@ cudaError_t launch_prim_x(const QuartetRec* recs, long long nrec, const ShellPai
 cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, const double* out, const long long* len,
                                      double* q, cudaStream_t stream);
 cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
-                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream);
+                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream,
+                               int block_elems);
 cudaError_t launch_symmetrize(const double* X, double* M, int n, cudaStream_t stream);
 cudaError_t launch_scatter_s8(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
                               const double* out, double* eri, cudaStream_t stream);
@@ -821,10 +822,15 @@ int cintx_plan_jk(CintxPlan* p, const double* dm, int nao, double* vj, double* v
   for (int64_t c = 0; c < (int64_t)p->chunks.size(); ++c) {
     int rc = cintx_plan_execute(p, c, p->d_stage, stream);
     if (rc) return rc;
-    if (launch_jk_contract(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc, p->d_stage, dm, nao, A, Bk, stream) !=
-        cudaSuccess) {
-      set_error(CINTX_STATUS_EXECUTION_FAILED, "J/K contraction launch failed");
-      return CINTX_STATUS_EXECUTION_FAILED;
+    // one contraction launch per class segment: small blocks one thread per quartet, others a warp
+    for (const Segment& sg : p->chunks[c].segs) {
+      const int n = nsph_or_cart(sg.li, p->sph) * nsph_or_cart(sg.lj, p->sph) * nsph_or_cart(sg.lk, p->sph) *
+                    nsph_or_cart(sg.ll, p->sph);
+      if (launch_jk_contract(p->d_recs + sg.rec0, sg.nrec, p->d_psh, p->d_aoloc, p->d_stage, dm, nao, A, Bk, stream,
+                             n) != cudaSuccess) {
+        set_error(CINTX_STATUS_EXECUTION_FAILED, "J/K contraction launch failed");
+        return CINTX_STATUS_EXECUTION_FAILED;
+      }
     }
   }
   if ((vj && launch_symmetrize(A, vj, nao, stream) != cudaSuccess) ||

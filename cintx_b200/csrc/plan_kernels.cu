@@ -210,6 +210,69 @@ __global__ void scatter_s8_kernel(const QuartetRec* __restrict__ recs, long long
   }
 }
 
+// As jk_contract_kernel for small blocks (all of one class, n = ni nj nk nl <= 32 elements): one
+// thread per quartet, so the many tiny blocks ((ss|ss), (ps|ss), ...) do not idle a warp each.
+__global__ void jk_contract_small_kernel(const QuartetRec* __restrict__ recs, long long nrec,
+                                         const int2* __restrict__ psh, const int* __restrict__ aoloc,
+                                         const double* __restrict__ out, const double* __restrict__ dm, int nao,
+                                         double* __restrict__ A, double* __restrict__ B) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nrec; r += (long long)gridDim.x * blockDim.x) {
+    const QuartetRec rec = recs[r];
+    const int2 ab = psh[rec.pij], cd = psh[rec.pkl];
+    const int i0 = aoloc[ab.x], j0 = aoloc[ab.y], k0 = aoloc[cd.x], l0 = aoloc[cd.y];
+    const int ni = aoloc[ab.x + 1] - i0, nj = aoloc[ab.y + 1] - j0;
+    const int nk = aoloc[cd.x + 1] - k0, nl = aoloc[cd.y + 1] - l0;
+    const double s = (ab.x == ab.y ? 0.5 : 1.0) * (cd.x == cd.y ? 0.5 : 1.0) * (rec.pij == rec.pkl ? 0.5 : 1.0);
+    const double* v = out + rec.out;
+    const int sj = ni, sk = ni * nj, sl = ni * nj * nk;
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        double tj = 0.0;  // A[i,j]
+        for (int l = 0; l < nl; ++l)
+          for (int k = 0; k < nk; ++k) tj += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(k0 + k) * nao + l0 + l];
+        if (A) atomicAdd(A + (size_t)(i0 + i) * nao + j0 + j, 2.0 * s * tj);
+      }
+    if (A)
+      for (int l = 0; l < nl; ++l)
+        for (int k = 0; k < nk; ++k) {
+          double t = 0.0;
+          for (int j = 0; j < nj; ++j)
+            for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + j0 + j];
+          atomicAdd(A + (size_t)(k0 + k) * nao + l0 + l, 2.0 * s * t);
+        }
+    if (B) {
+      for (int k = 0; k < nk; ++k) {
+        for (int i = 0; i < ni; ++i) {  // B[i,k] += s sum_jl v D[j,l]
+          double t = 0.0;
+          for (int l = 0; l < nl; ++l)
+            for (int j = 0; j < nj; ++j) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(j0 + j) * nao + l0 + l];
+          atomicAdd(B + (size_t)(i0 + i) * nao + k0 + k, s * t);
+        }
+        for (int j = 0; j < nj; ++j) {  // B[j,k] += s sum_il v D[i,l]
+          double t = 0.0;
+          for (int l = 0; l < nl; ++l)
+            for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + l0 + l];
+          atomicAdd(B + (size_t)(j0 + j) * nao + k0 + k, s * t);
+        }
+      }
+      for (int l = 0; l < nl; ++l) {
+        for (int i = 0; i < ni; ++i) {  // B[i,l] += s sum_jk v D[j,k]
+          double t = 0.0;
+          for (int k = 0; k < nk; ++k)
+            for (int j = 0; j < nj; ++j) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(j0 + j) * nao + k0 + k];
+          atomicAdd(B + (size_t)(i0 + i) * nao + l0 + l, s * t);
+        }
+        for (int j = 0; j < nj; ++j) {  // B[j,l] += s sum_ik v D[i,k]
+          double t = 0.0;
+          for (int k = 0; k < nk; ++k)
+            for (int i = 0; i < ni; ++i) t += v[i + j * sj + k * sk + l * sl] * dm[(size_t)(i0 + i) * nao + k0 + k];
+          atomicAdd(B + (size_t)(j0 + j) * nao + l0 + l, s * t);
+        }
+      }
+    }
+  }
+}
+
 // M[p,q] = X[p,q] + X[q,p] (n x n), for J = A + A^T and K = B + B^T.
 __global__ void symmetrize_kernel(const double* __restrict__ X, double* __restrict__ M, int n) {
   const long long total = (long long)n * n;
@@ -239,8 +302,15 @@ cudaError_t launch_block_absmax_sqrt(const QuartetRec* recs, long long nrec, con
 }
 
 cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
-                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream) {
+                               const double* out, const double* dm, int nao, double* A, double* B, cudaStream_t stream,
+                               int block_elems) {
   if (nrec <= 0) return cudaSuccess;
+  if (block_elems > 0 && block_elems <= 32) {
+    long long blocks = (nrec + 127) / 128;
+    if (blocks > 148LL * 64) blocks = 148LL * 64;
+    jk_contract_small_kernel<<<(unsigned)blocks, 128, 0, stream>>>(recs, nrec, psh, aoloc, out, dm, nao, A, B);
+    return cudaGetLastError();
+  }
   long long blocks = (nrec * 32 + 255) / 256;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   jk_contract_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, dm, nao, A, B);
