@@ -91,6 +91,8 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_autotune.restype = _i
     L.cintx_plan_use_tuned_shapes.argtypes = [_vp]
     L.cintx_plan_use_tuned_shapes.restype = _i
+    L.cintx_plan_set_shape.argtypes = [_vp, _i]
+    L.cintx_plan_set_shape.restype = _i
     L.cintx_plan_segment_lanes.argtypes = [_vp, _i64, _ip, _i]
     L.cintx_plan_segment_lanes.restype = _i
     L.cintx_plan_destroy.argtypes = [_vp]
@@ -379,6 +381,13 @@ class Plan:
         n = lib.cintx_plan_use_tuned_shapes(self.handle)
         if n < 0:
             _check(1)
+        return n
+
+    def set_shape(self, variant: int) -> int:
+        """Runs every segment in launch-shape variant `variant` (0 = default shape)."""
+        n = lib.cintx_plan_set_shape(self.handle, variant)
+        if n < 0:
+            _check(last_error()[0])
         return n
 
     def segment_lanes(self, chunk: int) -> np.ndarray:

@@ -152,6 +152,19 @@ __device__ __forceinline__ void group_sync(int group) {
   }
 }
 
+// Barrier of one quartet's lanes.  Sliced shapes spread a quartet's S lanes over S warps (one
+// lane per warp, see eri4c_kernel), so their S warps meet at a named barrier per set of S warps.
+template <int S, bool SLICE, int BLOCK>
+__device__ __forceinline__ void quartet_sync(int group) {
+  if constexpr (SLICE && BLOCK == 32 * S) {
+    __syncthreads();
+  } else if constexpr (SLICE) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / (32 * S))), "r"(32 * S) : "memory");
+  } else {
+    group_sync<S>(group);
+  }
+}
+
 // 2D recurrence for one (axis, root) followed by the horizontal transfers; writes
 // I[i + NI*(j + NJ*(k + NK*l))] to dst (stride 1).
 template <int LI, int LJ, int LK, int LL, class R = double>
@@ -429,8 +442,14 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];
-  const int group = threadIdx.x / S;
-  const int lane = threadIdx.x % S;
+  // Sliced shapes run a different compile-time instance of the primitive loop on each of a
+  // quartet's S lanes.  Lanes of one quartet therefore sit in S different warps: a set of S warps
+  // holds 32 quartets, warp w of the set runs slice w for all of them (no divergence inside a
+  // warp), and the set meets at a named barrier for the transform stages.  Other shapes keep a
+  // quartet's lanes adjacent within a warp.
+  static_assert(!SLICE || (SH::BLOCK % (32 * S) == 0 && !SH::GLOBAL_BUF), "sliced shape layout");
+  const int group = SLICE ? (int)(threadIdx.x / (32 * S)) * 32 + (int)(threadIdx.x & 31) : (int)threadIdx.x / S;
+  const int lane = SLICE ? (int)(threadIdx.x / 32) % S : (int)threadIdx.x % S;
   char* sgb = reinterpret_cast<char*>(smem + SH::TABLE_DOUBLES) + group * SH::B_GROUP;
   double* sg = reinterpret_cast<double*>(sgb);  // transform buffers after the primitive loop
   double* s_roots = sg;                         // t2[NR], w[NR]
@@ -447,7 +466,13 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   LaneTuples<SH> lt;
   decode_tuples<SH, LJ, LK, LL>(lt, lane);
 
-  for (int q = blockIdx.x * SH::Q + group; q < nrec; q += gridDim.x * SH::Q) {
+  // q = blockIdx.x * Q + group; in sliced shapes every thread of a set runs the trip count of the
+  // set's first quartet (the set shares barriers) and lanes past the end only take part in them
+  const int qfirst = SLICE ? (int)blockIdx.x * SH::Q + (group & ~31) : (int)blockIdx.x * SH::Q + group;
+  for (int qb = qfirst; qb < nrec; qb += gridDim.x * SH::Q) {
+    const int qv = SLICE ? qb + (group & 31) : qb;
+    const bool live = !SLICE || qv < nrec;
+    const int q = live ? qv : nrec - 1;
     const QuartetRec rec = recs[q];
     // precomputed roots of this quartet's primitive quartets ([b][a][2*NR]), or table roots
     const double* rb = rootbuf ? rootbuf + rootbase[q] : nullptr;
@@ -465,7 +490,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     } else if constexpr (SLICE) {
       // each lane runs the register path for its own tuple slice (lane + S*k)
       static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
-        if (lane == decltype(j)::value)
+        if (live && lane == decltype(j)::value)
           prim_loop_one_lane<LI, LJ, LK, LL, SH, R, decltype(j)::value>(pij, pkl, prims, rys, nullptr, expcutoff,
                                                                          prim_eps, rb, lt, acc);
       });
@@ -623,7 +648,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           }
         }
       }
-      group_sync<S>(group);
+      quartet_sync<S, SLICE, SH::BLOCK>(group);
       // stage j: bufA[mi + MI*(fj + NFJ*(fk + NFK*fl))] -> bufB[mi + MI*(mj + MJ*(fk + NFK*fl))]
       const double* cur = bufA;
       if constexpr (SPH && LJ >= 2) {
@@ -637,7 +662,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           for (int z = 0; z < row.nnz; ++z) v += row.c[z] * bufA[mi + SH::MI * (row.f[z] + SH::NFJ * rest)];
           bufB[o] = v;
         }
-        group_sync<S>(group);
+        quartet_sync<S, SLICE, SH::BLOCK>(group);
         cur = bufB;
       }
       // stage k: cur[mi + MI*(mj + MJ*(fk + NFK*fl))] -> nxt[mi + MI*(mj + MJ*(mk + MK*fl))]
@@ -654,7 +679,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
             v += row.c[z] * cur[mij + SH::MI * SH::MJ * (row.f[z] + SH::NFK * fl)];
           nxt[o] = v;
         }
-        group_sync<S>(group);
+        quartet_sync<S, SLICE, SH::BLOCK>(group);
         cur = nxt;
       }
       // stage l + store: cur[mijk + MIJK*fl] -> out
@@ -675,10 +700,10 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           } else {
             v = cur[mijk + MIJK * ml];
           }
-          obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
+          if (live) obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
         }
       }
-      group_sync<S>(group);
+      quartet_sync<S, SLICE, SH::BLOCK>(group);
     }
   }
 }

@@ -1069,6 +1069,29 @@ int cintx_plan_use_tuned_shapes(CintxPlan* p) {
   return applied;
 }
 
+int cintx_plan_set_shape(CintxPlan* p, int variant) {
+  clear_error();
+  if (!p) {
+    set_error(CINTX_STATUS_NULL_POINTER, "plan must not be NULL");
+    return -1;
+  }
+  if (variant < 0 || variant >= kLaunchVariants) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "launch-shape variant out of range");
+    return -1;
+  }
+  int changed = 0;
+  for (Chunk& ch : p->chunks)
+    for (Segment& sg : ch.segs) {
+      changed += sg.variant != variant;
+      sg.variant = variant;
+    }
+  if (changed && p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  return changed;
+}
+
 int cintx_plan_segment_lanes(const CintxPlan* p, int64_t chunk, int* lanes, int cap) {
   if (!p || chunk < 0 || chunk >= (int64_t)p->chunks.size()) return -1;
   const std::vector<Segment>& segs = p->chunks[chunk].segs;

@@ -237,6 +237,34 @@ def test_autotuned_launch_shapes_give_the_same_integrals(cx):
         plan.close()
 
 
+def test_every_launch_shape_gives_the_same_integrals(cx):
+    """Each launch-shape variant (lane counts, register caps, the sliced shapes whose lanes sit in
+    separate warps) run on every class of an s/p/d/f molecule matches the default shape."""
+    mol = M.random_molecule("spdf10", 11, 10, 9.0, with_f=True)
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-12, sph=True, max_chunk_doubles=1 << 24)
+        st = plan.stats
+        s = torch.cuda.current_stream().cuda_stream
+        buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
+        outs = {}
+        for v in range(6):
+            assert plan.set_shape(v) >= 0
+            res = []
+            for c in range(st.nchunks):
+                buf.zero_()
+                plan.execute(buf.data_ptr(), chunk=c, stream=s)
+                torch.cuda.synchronize()
+                res.append(buf[:plan.chunk_size(c)].cpu().numpy())
+            outs[v] = np.concatenate(res)
+        assert np.abs(outs[0]).max() > 0
+        for v in range(1, 6):
+            assert close(outs[v], outs[0]), v
+        with pytest.raises(cx.CintxError):
+            plan.set_shape(6)
+        plan.close()
+
+
 def test_graph_replay_matches_direct_execution(cx):
     mol = M.mol40()
     import torch
