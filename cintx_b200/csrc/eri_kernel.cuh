@@ -61,22 +61,26 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // register cap of multi-lane shapes (variant 0 is the default shape, used by plans that are not
 // autotuned).  A 255-register cap halves the resident blocks but removes the spills that the
 // 128-register cap forces on most d/f/g multi-lane classes.
-// Variants 4 and 5 ("sliced") run a multi-lane class without any barrier inside the primitive
+// Variants 4, 5 and 6 ("sliced") run a multi-lane class without any barrier inside the primitive
 // loop: every lane evaluates the roots and all 3*NR recurrences itself in registers and
 // accumulates its own slice of (j,k,l) tuples (redundant FP64 work for no shared-memory
 // hand-offs); the lanes meet only for the cartesian-to-spherical stages.
-constexpr int kNumVariants = 6;
+constexpr int kNumVariants = 7;
 __host__ __device__ constexpr int variant_acc(int v) {
-  return v == 1 || v == 5 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
+  return v == 1 || v == 5 || v == 6 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
 }
 __host__ __device__ constexpr int variant_regs(int v) { return v == 0 || v == 2 ? 128 : 255; }
-__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5; }
-// a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (each
-// lane's slice is a separate compile-time instance of the register path)
+__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5 || v == 6; }
+// a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (variants
+// 4, 5), or to 8 lanes whose tables hold at most 108 values (variant 6: a lane keeps only the
+// entries its own tuples read; each lane's slice is a separate compile-time instance of the
+// register path)
 __host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int v) {
-  return variant_sliced(v) && pick_threads(li, lj, lk, ll, variant_acc(v)) >= 2 &&
-         pick_threads(li, lj, lk, ll, variant_acc(v)) <= 4 &&
-         3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= (v == 4 ? 48 : 72);
+  return v == 6 ? pick_threads(li, lj, lk, ll, variant_acc(v)) == 8 &&
+                      3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= 108
+                : variant_sliced(v) && pick_threads(li, lj, lk, ll, variant_acc(v)) >= 2 &&
+                      pick_threads(li, lj, lk, ll, variant_acc(v)) <= 4 &&
+                      3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= (v == 4 ? 48 : 72);
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
@@ -124,7 +128,10 @@ struct EriShape {
              : (SLICE ? (GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8)
                       : cmax(B_ROOTS + B_G + B_SCR, GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8));
   static constexpr int B_GROUP = (B_GROUP_RAW + 15) & ~15;
-  static constexpr int BLOCK = S >= 128 ? S : 128;
+  static constexpr int BLOCK = SLICE ? cmax(128, 32 * S) : (S >= 128 ? S : 128);
+  // 8-lane sliced shapes loop over the roots instead of unrolling them (eight compile-time
+  // slices of NR unrolled root bodies made the compile time explode)
+  static constexpr bool ROLL_ROOTS = SLICE && S >= 8;
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : (65536 / (BLOCK * REGS) > 0 ? 65536 / (BLOCK * REGS) : 1);
@@ -391,8 +398,7 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
 #pragma unroll
             for (int f2 = 0; f2 < NFI; ++f2) part[k2][f2] = (R)0;
         }
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
+        auto root_body = [&](const int r) {
           R gg[3 * GSZ];
           const double rt_aa = t2[r] * inv_aijkl;
           const double b00 = 0.5 * rt_aa;
@@ -418,6 +424,13 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
               else part[k][fi] = fmaf(gg[ix] * gg[iy], gg[iz], part[k][fi]);
             }
           });
+        };
+        if constexpr (SH::ROLL_ROOTS) {  // t2, w then live in local memory: two loads per root
+#pragma unroll 1
+          for (int r = 0; r < NR; ++r) root_body(r);
+        } else {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) root_body(r);
         }
         if constexpr (!std::is_same<R, double>::value) {
 #pragma unroll
@@ -447,7 +460,8 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   // holds 32 quartets, warp w of the set runs slice w for all of them (no divergence inside a
   // warp), and the set meets at a named barrier for the transform stages.  Other shapes keep a
   // quartet's lanes adjacent within a warp.
-  static_assert(!SLICE || (SH::BLOCK % (32 * S) == 0 && !SH::GLOBAL_BUF), "sliced shape layout");
+  static_assert(!SLICE || (SH::BLOCK % (32 * S) == 0 && !SH::GLOBAL_BUF && SH::SMEM_BYTES <= 227 * 1024),
+                "sliced shape layout");
   const int group = SLICE ? (int)(threadIdx.x / (32 * S)) * 32 + (int)(threadIdx.x & 31) : (int)threadIdx.x / S;
   const int lane = SLICE ? (int)(threadIdx.x / 32) % S : (int)threadIdx.x % S;
   char* sgb = reinterpret_cast<char*>(smem + SH::TABLE_DOUBLES) + group * SH::B_GROUP;

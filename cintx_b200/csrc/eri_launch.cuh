@@ -129,6 +129,12 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
               done = true;
             }
           }
+          if constexpr (sliced_ok(LI, LJ, k, l, 6)) {
+            if (!done && a.variant == 6) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(6), variant_regs(6), true>(a);
+              done = true;
+            }
+          }
           if (!done) err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }
