@@ -8,6 +8,8 @@
 // 1e10 quartets.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -987,6 +989,9 @@ int cintx_plan_autotune(CintxPlan* p, int64_t chunk, double* out_dev, void* stre
   // quartet, register cap) and needs device scratch only if the default shape does, so graphs
   // stay possible
   std::map<std::tuple<int, int, int, int, int>, int> best;
+  // CINTX_AUTOTUNE_LOG=1 prints every timing to stderr
+  const char* tl = getenv("CINTX_AUTOTUNE_LOG");
+  const bool tune_log = tl && tl[0] && tl[0] != '0';
   for (const auto& tg : target) {
     const auto& key = tg.first;
     const Segment& sg0 = p->chunks[tg.second.first].segs[tg.second.second];
@@ -1013,6 +1018,10 @@ int cintx_plan_autotune(CintxPlan* p, int64_t chunk, double* out_dev, void* stre
       }
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
+      if (tune_log)
+        fprintf(stderr, "cintx autotune (%d%d|%d%d)%s variant %d lanes %d: %.4f ms\n", sg0.li, sg0.lj, sg0.lk, sg0.ll,
+                sg0.fp32 ? " fp32" : "", v, variant_lanes(sg0.li, sg0.lj, sg0.lk, sg0.ll, p->sph, sg0.fp32, v),
+                ms / reps);
       if (ms < best_ms) {
         best_ms = ms;
         best_v = v;
