@@ -40,7 +40,8 @@ int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int varia
   if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   const int s = pick_threads(li, lj, lk, ll, variant_acc(variant));
   if (s == 1) return 1;  // one-lane shapes take no register cap
-  return (variant_sliced(variant) ? 1 << 20 : 0) + s * 1024 + variant_regs(variant);
+  return (variant_sliced(variant) ? 1 << 20 : 0) + (variant_roll(variant) ? 1 << 21 : 0) + s * 1024 +
+         variant_regs(variant);
 }
 
 bool class_needs_scratch(int li, int lj, int lk, int ll, bool sph, int variant) {

@@ -65,12 +65,15 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // loop: every lane evaluates the roots and all 3*NR recurrences itself in registers and
 // accumulates its own slice of (j,k,l) tuples (redundant FP64 work for no shared-memory
 // hand-offs); the lanes meet only for the cartesian-to-spherical stages.
-constexpr int kNumVariants = 7;
+// Variant 7 is variant 5 with the root loop rolled (a quarter to a fifth of the code per slice:
+// the slices' bodies compete for the instruction cache).
+constexpr int kNumVariants = 8;
 __host__ __device__ constexpr int variant_acc(int v) {
-  return v == 1 || v == 5 || v == 6 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
+  return v == 1 || v == 5 || v == 6 || v == 7 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
 }
+__host__ __device__ constexpr bool variant_roll(int v) { return v == 7; }
 __host__ __device__ constexpr int variant_regs(int v) { return v == 0 || v == 2 ? 128 : 255; }
-__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5 || v == 6; }
+__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5 || v == 6 || v == 7; }
 // a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (variants
 // 4, 5), or to 8 lanes whose tables hold at most 108 values (variant 6: a lane keeps only the
 // entries its own tuples read; each lane's slice is a separate compile-time instance of the
@@ -84,7 +87,7 @@ __host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false>
+          bool SLICE = false, bool ROLL = false>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -131,7 +134,7 @@ struct EriShape {
   static constexpr int BLOCK = SLICE ? cmax(128, 32 * S) : (S >= 128 ? S : 128);
   // 8-lane sliced shapes loop over the roots instead of unrolling them (eight compile-time
   // slices of NR unrolled root bodies made the compile time explode)
-  static constexpr bool ROLL_ROOTS = SLICE && S >= 8;
+  static constexpr bool ROLL_ROOTS = SLICE && (S >= 8 || ROLL);
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : (65536 / (BLOCK * REGS) > 0 ? 65536 / (BLOCK * REGS) : 1);
@@ -444,14 +447,14 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>::BLOCK,
-                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>::MINB)
+          bool SLICE = false, bool ROLL = false>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>::BLOCK,
+                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
                  double prim_eps, const double* __restrict__ rootbuf, const long long* __restrict__ rootbase) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];

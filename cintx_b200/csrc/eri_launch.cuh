@@ -38,11 +38,11 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 int device_sm_count();
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false>
+          bool SLICE = false, bool ROLL = false>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -132,6 +132,12 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
           if constexpr (sliced_ok(LI, LJ, k, l, 6)) {
             if (!done && a.variant == 6) {
               err = launch_eri<LI, LJ, k, l, true, double, variant_acc(6), variant_regs(6), true>(a);
+              done = true;
+            }
+          }
+          if constexpr (sliced_ok(LI, LJ, k, l, 7)) {
+            if (!done && a.variant == 7) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(7), variant_regs(7), true, true>(a);
               done = true;
             }
           }
