@@ -65,15 +65,15 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // loop: every lane evaluates the roots and all 3*NR recurrences itself in registers and
 // accumulates its own slice of (j,k,l) tuples (redundant FP64 work for no shared-memory
 // hand-offs); the lanes meet only for the cartesian-to-spherical stages.
-// Variant 7 is variant 5 with the root loop rolled (a quarter to a fifth of the code per slice:
-// the slices' bodies compete for the instruction cache).
-constexpr int kNumVariants = 8;
+// Variants 7 and 8 are variants 5 and 4 with the root loop rolled (a quarter to a fifth of the
+// code per slice: the slices' bodies compete for the instruction cache).
+constexpr int kNumVariants = 9;
 __host__ __device__ constexpr int variant_acc(int v) {
-  return v == 1 || v == 5 || v == 6 || v == 7 ? 48 : (v == 2 ? 12 : (v == 4 ? 32 : 24));
+  return v == 1 || v == 5 || v == 6 || v == 7 ? 48 : (v == 2 ? 12 : (v == 4 || v == 8 ? 32 : 24));
 }
-__host__ __device__ constexpr bool variant_roll(int v) { return v == 7; }
+__host__ __device__ constexpr bool variant_roll(int v) { return v == 7 || v == 8; }
 __host__ __device__ constexpr int variant_regs(int v) { return v == 0 || v == 2 ? 128 : 255; }
-__host__ __device__ constexpr bool variant_sliced(int v) { return v == 4 || v == 5 || v == 6 || v == 7; }
+__host__ __device__ constexpr bool variant_sliced(int v) { return v >= 4 && v <= 8; }
 // a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (variants
 // 4, 5), or to 8 lanes whose tables hold at most 108 values (variant 6: a lane keeps only the
 // entries its own tuples read; each lane's slice is a separate compile-time instance of the
@@ -83,7 +83,7 @@ __host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int
                       3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= 108
                 : variant_sliced(v) && pick_threads(li, lj, lk, ll, variant_acc(v)) >= 2 &&
                       pick_threads(li, lj, lk, ll, variant_acc(v)) <= 4 &&
-                      3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= (v == 4 ? 48 : 72);
+                      3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= (v == 4 || v == 8 ? 48 : 72);
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
@@ -130,7 +130,11 @@ struct EriShape {
       S == 1 ? 0
              : (SLICE ? (GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8)
                       : cmax(B_ROOTS + B_G + B_SCR, GLOBAL_BUF ? 0 : (SM_BUFA + SM_BUFB) * 8));
-  static constexpr int B_GROUP = (B_GROUP_RAW + 15) & ~15;
+  // sliced shapes: the 32 lanes of a warp belong to 32 groups and read the same offset of their
+  // transform buffers, so the group stride is an odd number of doubles (no bank conflicts within
+  // a 16-lane phase of an 8-byte access); other shapes keep 16-byte group alignment
+  static constexpr int B_GROUP = SLICE ? ((B_GROUP_RAW + 7) / 8 + ((B_GROUP_RAW + 7) / 8 % 2 == 0 ? 1 : 0)) * 8
+                                       : (B_GROUP_RAW + 15) & ~15;
   static constexpr int BLOCK = SLICE ? cmax(128, 32 * S) : (S >= 128 ? S : 128);
   // 8-lane sliced shapes loop over the roots instead of unrolling them (eight compile-time
   // slices of NR unrolled root bodies made the compile time explode)

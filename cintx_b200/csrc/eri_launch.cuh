@@ -141,6 +141,12 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
               done = true;
             }
           }
+          if constexpr (sliced_ok(LI, LJ, k, l, 8)) {
+            if (!done && a.variant == 8) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(8), variant_regs(8), true, true>(a);
+              done = true;
+            }
+          }
           if (!done) err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }
