@@ -32,7 +32,7 @@ static_assert(kNumVariants == kLaunchVariants, "variant count differs between ke
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
   if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
-  return pick_threads(li, lj, lk, ll, variant_acc(variant));
+  return pick_threads(li, lj, lk, ll, variant_acc(variant)) / variant_passes(variant);
 }
 
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
@@ -40,7 +40,8 @@ int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int varia
   if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   const int s = pick_threads(li, lj, lk, ll, variant_acc(variant));
   if (s == 1) return 1;  // one-lane shapes take no register cap
-  return (variant_sliced(variant) ? 1 << 20 : 0) + (variant_roll(variant) ? 1 << 21 : 0) + s * 1024 +
+  return (variant_sliced(variant) ? 1 << 20 : 0) + (variant_roll(variant) ? 1 << 21 : 0) +
+         (variant_passes(variant) > 1 ? 1 << 22 : 0) + s * 1024 +
          variant_regs(variant);
 }
 

@@ -66,20 +66,22 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // accumulates its own slice of (j,k,l) tuples (redundant FP64 work for no shared-memory
 // hand-offs); the lanes meet only for the cartesian-to-spherical stages.
 // Variants 7 and 8 are variants 5 and 4 with the root loop rolled (a quarter to a fifth of the
-// code per slice: the slices' bodies compete for the instruction cache).
-constexpr int kNumVariants = 9;
+// code per slice: the slices' bodies compete for the instruction cache).  Variant 9 runs the eight
+// slices of variant 6 on four warps, two slices after one another per warp.
+constexpr int kNumVariants = 10;
 __host__ __device__ constexpr int variant_acc(int v) {
-  return v == 1 || v == 5 || v == 6 || v == 7 ? 48 : (v == 2 ? 12 : (v == 4 || v == 8 ? 32 : 24));
+  return v == 1 || v == 5 || v == 6 || v == 7 || v == 9 ? 48 : (v == 2 ? 12 : (v == 4 || v == 8 ? 32 : 24));
 }
+__host__ __device__ constexpr int variant_passes(int v) { return v == 9 ? 2 : 1; }
 __host__ __device__ constexpr bool variant_roll(int v) { return v == 7 || v == 8; }
 __host__ __device__ constexpr int variant_regs(int v) { return v == 0 || v == 2 ? 128 : 255; }
-__host__ __device__ constexpr bool variant_sliced(int v) { return v >= 4 && v <= 8; }
+__host__ __device__ constexpr bool variant_sliced(int v) { return v >= 4 && v <= 9; }
 // a sliced shape applies to 2..4 lanes whose three recurrence tables fit in registers (variants
 // 4, 5), or to 8 lanes whose tables hold at most 108 values (variant 6: a lane keeps only the
 // entries its own tuples read; each lane's slice is a separate compile-time instance of the
 // register path)
 __host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int v) {
-  return v == 6 ? pick_threads(li, lj, lk, ll, variant_acc(v)) == 8 &&
+  return v == 6 || v == 9 ? pick_threads(li, lj, lk, ll, variant_acc(v)) == 8 &&
                       3 * (li + 1) * (lj + 1) * (lk + 1) * (ll + 1) <= 108
                 : variant_sliced(v) && pick_threads(li, lj, lk, ll, variant_acc(v)) >= 2 &&
                       pick_threads(li, lj, lk, ll, variant_acc(v)) <= 4 &&
@@ -87,7 +89,7 @@ __host__ __device__ constexpr bool sliced_ok(int li, int lj, int lk, int ll, int
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false, bool ROLL = false>
+          bool SLICE = false, bool ROLL = false, int PASSES = 1>
 struct EriShape {
   static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
   static constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1, NL = LL + 1;
@@ -135,14 +137,16 @@ struct EriShape {
   // a 16-lane phase of an 8-byte access); other shapes keep 16-byte group alignment
   static constexpr int B_GROUP = SLICE ? ((B_GROUP_RAW + 7) / 8 + ((B_GROUP_RAW + 7) / 8 % 2 == 0 ? 1 : 0)) * 8
                                        : (B_GROUP_RAW + 15) & ~15;
-  static constexpr int BLOCK = SLICE ? cmax(128, 32 * S) : (S >= 128 ? S : 128);
+  // threads per quartet: S, or for sliced shapes run in PASSES passes, S / PASSES warps' lanes
+  static constexpr int LANES = SLICE ? S / PASSES : S;
+  static constexpr int BLOCK = SLICE ? cmax(128, 32 * LANES) : (S >= 128 ? S : 128);
   // 8-lane sliced shapes loop over the roots instead of unrolling them (eight compile-time
   // slices of NR unrolled root bodies made the compile time explode)
   static constexpr bool ROLL_ROOTS = SLICE && (S >= 8 || ROLL);
   // resident blocks requested from the register allocator: <= 128 registers per thread for the
   // multi-lane kernels (their stalls are latency bound and need warps)
   static constexpr int MINB = S == 1 ? 1 : (65536 / (BLOCK * REGS) > 0 ? 65536 / (BLOCK * REGS) : 1);
-  static constexpr int Q = BLOCK / S;
+  static constexpr int Q = BLOCK / LANES;
   // one-lane classes of low order stage their root-table block in shared memory: the lanes'
   // scattered coefficient loads then cost shared-memory wavefronts instead of L1 sectors
   // (multi-lane groups evaluate each root once per group; a per-block copy there costs more
@@ -451,14 +455,14 @@ __device__ __forceinline__ void prim_loop_one_lane(const ShellPair& pij, const S
 }
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false, bool ROLL = false>
-__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>::BLOCK,
-                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>::MINB)
+          bool SLICE = false, bool ROLL = false, int PASSES = 1>
+__global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>::BLOCK,
+                                  EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>::MINB)
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
                  double prim_eps, const double* __restrict__ rootbuf, const long long* __restrict__ rootbase) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
   extern __shared__ __align__(16) double smem[];
@@ -466,11 +470,14 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   // quartet's S lanes.  Lanes of one quartet therefore sit in S different warps: a set of S warps
   // holds 32 quartets, warp w of the set runs slice w for all of them (no divergence inside a
   // warp), and the set meets at a named barrier for the transform stages.  Other shapes keep a
-  // quartet's lanes adjacent within a warp.
-  static_assert(!SLICE || (SH::BLOCK % (32 * S) == 0 && !SH::GLOBAL_BUF && SH::SMEM_BYTES <= 227 * 1024),
+  // quartet's lanes adjacent within a warp.  With PASSES == 2 a set has S/2 warps and warp w runs
+  // slices w and w + S/2 one after the other.
+  constexpr int LN = SH::LANES;
+  static_assert(!SLICE || (SH::BLOCK % (32 * LN) == 0 && S % PASSES == 0 && !SH::GLOBAL_BUF &&
+                           SH::SMEM_BYTES <= 227 * 1024),
                 "sliced shape layout");
-  const int group = SLICE ? (int)(threadIdx.x / (32 * S)) * 32 + (int)(threadIdx.x & 31) : (int)threadIdx.x / S;
-  const int lane = SLICE ? (int)(threadIdx.x / 32) % S : (int)threadIdx.x % S;
+  const int group = SLICE ? (int)(threadIdx.x / (32 * LN)) * 32 + (int)(threadIdx.x & 31) : (int)threadIdx.x / S;
+  const int lane = SLICE ? (int)(threadIdx.x / 32) % LN : (int)threadIdx.x % S;
   char* sgb = reinterpret_cast<char*>(smem + SH::TABLE_DOUBLES) + group * SH::B_GROUP;
   double* sg = reinterpret_cast<double*>(sgb);  // transform buffers after the primitive loop
   double* s_roots = sg;                         // t2[NR], w[NR]
@@ -511,9 +518,32 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     } else if constexpr (SLICE) {
       // each lane runs the register path for its own tuple slice (lane + S*k)
       static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
-        if (live && lane == decltype(j)::value)
-          prim_loop_one_lane<LI, LJ, LK, LL, SH, R, decltype(j)::value>(pij, pkl, prims, rys, nullptr, expcutoff,
-                                                                         prim_eps, rb, lt, acc);
+        constexpr int sl = decltype(j)::value;
+        if (live && lane == sl % LN) {
+          prim_loop_one_lane<LI, LJ, LK, LL, SH, R, sl>(pij, pkl, prims, rys, nullptr, expcutoff, prim_eps, rb, lt,
+                                                        acc);
+          if constexpr (PASSES > 1) {
+            // stage i of this slice now: the next pass reuses the accumulators
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+              const int t = sl + S * k;
+              if (t < SH::NTUP) {
+#pragma unroll
+                for (int mi = 0; mi < SH::MI; ++mi) {
+                  double v = 0.0;
+#pragma unroll
+                  for (int fi = 0; fi < NFI; ++fi) {
+                    const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+                    if (c != 0.0) v += c * acc[k][fi];
+                  }
+                  sg[mi + SH::MI * t] = v;
+                }
+              }
+#pragma unroll
+              for (int fi = 0; fi < NFI; ++fi) acc[k][fi] = 0.0;
+            }
+          }
+        }
       });
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
@@ -652,11 +682,12 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     } else {
       double* bufA = SH::GLOBAL_BUF ? gscratch + (size_t)blockIdx.x * SH::GBUF_PER_BLOCK : sg;
       double* bufB = bufA + SH::SM_BUFA;
-      // stage i in registers -> bufA[mi + MI * t], t = fj + NFJ*(fk + NFK*fl)
+      // stage i in registers -> bufA[mi + MI * t], t = fj + NFJ*(fk + NFK*fl) (two-pass sliced
+      // shapes stored it after each pass)
 #pragma unroll
       for (int k = 0; k < TPT; ++k) {
         const int t = lane + S * k;
-        if (t < SH::NTUP) {
+        if (PASSES == 1 && t < SH::NTUP) {
 #pragma unroll
           for (int mi = 0; mi < SH::MI; ++mi) {
             double v = 0.0;
@@ -669,12 +700,12 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           }
         }
       }
-      quartet_sync<S, SLICE, SH::BLOCK>(group);
+      quartet_sync<LN, SLICE, SH::BLOCK>(group);
       // stage j: bufA[mi + MI*(fj + NFJ*(fk + NFK*fl))] -> bufB[mi + MI*(mj + MJ*(fk + NFK*fl))]
       const double* cur = bufA;
       if constexpr (SPH && LJ >= 2) {
         constexpr int n = SH::MI * SH::MJ * SH::NFK * SH::NFL;
-        for (int o = lane; o < n; o += S) {
+        for (int o = lane; o < n; o += LN) {
           const int mi = o % SH::MI;
           const int mj = (o / SH::MI) % SH::MJ;
           const int rest = o / (SH::MI * SH::MJ);
@@ -683,14 +714,14 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           for (int z = 0; z < row.nnz; ++z) v += row.c[z] * bufA[mi + SH::MI * (row.f[z] + SH::NFJ * rest)];
           bufB[o] = v;
         }
-        quartet_sync<S, SLICE, SH::BLOCK>(group);
+        quartet_sync<LN, SLICE, SH::BLOCK>(group);
         cur = bufB;
       }
       // stage k: cur[mi + MI*(mj + MJ*(fk + NFK*fl))] -> nxt[mi + MI*(mj + MJ*(mk + MK*fl))]
       if constexpr (SPH && LK >= 2) {
         double* nxt = (cur == bufA) ? bufB : bufA;
         constexpr int n = SH::MI * SH::MJ * SH::MK * SH::NFL;
-        for (int o = lane; o < n; o += S) {
+        for (int o = lane; o < n; o += LN) {
           const int mij = o % (SH::MI * SH::MJ);
           const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
           const int fl = o / (SH::MI * SH::MJ * SH::MK);
@@ -700,14 +731,14 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
             v += row.c[z] * cur[mij + SH::MI * SH::MJ * (row.f[z] + SH::NFK * fl)];
           nxt[o] = v;
         }
-        quartet_sync<S, SLICE, SH::BLOCK>(group);
+        quartet_sync<LN, SLICE, SH::BLOCK>(group);
         cur = nxt;
       }
       // stage l + store: cur[mijk + MIJK*fl] -> out
       {
         constexpr int n = SH::NOUT;
         constexpr int MIJK = SH::MI * SH::MJ * SH::MK;
-        for (int o = lane; o < n; o += S) {
+        for (int o = lane; o < n; o += LN) {
           const int mi = o % SH::MI;
           const int mj = (o / SH::MI) % SH::MJ;
           const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
@@ -724,7 +755,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
           if (live) obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
         }
       }
-      quartet_sync<S, SLICE, SH::BLOCK>(group);
+      quartet_sync<LN, SLICE, SH::BLOCK>(group);
     }
   }
 }

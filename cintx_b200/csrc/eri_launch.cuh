@@ -38,11 +38,11 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 int device_sm_count();
 
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
-          bool SLICE = false, bool ROLL = false>
+          bool SLICE = false, bool ROLL = false, int PASSES = 1>
 cudaError_t launch_eri(const LaunchArgs& a) {
-  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
+  using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>;
   if (a.query) return SH::GLOBAL_BUF ? cudaErrorNotSupported : cudaSuccess;
-  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL>;
+  auto kern = eri4c_kernel<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>;
   static int attr_done[64];
   int dev = 0;
   cudaGetDevice(&dev);
@@ -144,6 +144,13 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
           if constexpr (sliced_ok(LI, LJ, k, l, 8)) {
             if (!done && a.variant == 8) {
               err = launch_eri<LI, LJ, k, l, true, double, variant_acc(8), variant_regs(8), true, true>(a);
+              done = true;
+            }
+          }
+          if constexpr (sliced_ok(LI, LJ, k, l, 9)) {
+            if (!done && a.variant == 9) {
+              err = launch_eri<LI, LJ, k, l, true, double, variant_acc(9), variant_regs(9), true, true,
+                               variant_passes(9)>(a);
               done = true;
             }
           }

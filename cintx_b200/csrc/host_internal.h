@@ -148,6 +148,6 @@ cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, 
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
 // Distinct launch shape of a variant (lanes and register cap), for telling variants apart.
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-constexpr int kLaunchVariants = 9;
+constexpr int kLaunchVariants = 10;
 
 }  // namespace cintx

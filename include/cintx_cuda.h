@@ -259,7 +259,7 @@ CINTX_API int cintx_plan_autotune(CintxPlan *plan, int64_t chunk, double *out_de
  * (any plan) to this plan's matching classes; returns the number of segments changed (or -1).
  * A graph captured earlier is released when anything changed. */
 CINTX_API int cintx_plan_use_tuned_shapes(CintxPlan *plan);
-/* Sets the launch-shape variant (0..8) of every segment, for tests and tuning scripts; a class
+/* Sets the launch-shape variant (0..9) of every segment, for tests and tuning scripts; a class
  * that the variant does not apply to runs its default shape.  Returns the number of segments
  * changed (or -1).  A graph captured earlier is released when anything changed. */
 CINTX_API int cintx_plan_set_shape(CintxPlan *plan, int variant);

@@ -248,7 +248,7 @@ def test_every_launch_shape_gives_the_same_integrals(cx):
         s = torch.cuda.current_stream().cuda_stream
         buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
         outs = {}
-        for v in range(9):
+        for v in range(10):
             assert plan.set_shape(v) >= 0
             res = []
             for c in range(st.nchunks):
@@ -258,10 +258,10 @@ def test_every_launch_shape_gives_the_same_integrals(cx):
                 res.append(buf[:plan.chunk_size(c)].cpu().numpy())
             outs[v] = np.concatenate(res)
         assert np.abs(outs[0]).max() > 0
-        for v in range(1, 9):
+        for v in range(1, 10):
             assert close(outs[v], outs[0]), v
         with pytest.raises(cx.CintxError):
-            plan.set_shape(9)
+            plan.set_shape(10)
         plan.close()
 
 
