@@ -9,14 +9,19 @@ timed region; L2 is flushed (a 512 MiB write) between timed steps outside the st
              launching stream), max over ranks
   e2e        the same metric through the C ABI from host arrays: optimizer build (host -> device
              basis and pair tables), screened plan, execution and the device -> host copy of every
-             chunk's output into pinned host memory, every step
+             chunk's output into pinned host memory, every step (max over ranks of each rank's
+             time, every rank evaluating its own chunks)
   roofline   the kernel class with the largest device time in one profiled step: algorithmic FP64
              flops (the plan's flop model) / its event time, against the FP64 FMA peak measured by
              a probe kernel on the same GPU in the same run
+  error_vs_libcint  the tuned output of a class-stratified sample of the sweep (up to 2000
+             quartets per class) against libcint 6.1.3 built from the reference sources
   cpu_baseline  libcint 6.1.3 built from the reference sources (oracle/_ref), all host cores,
-             on a seeded uniform sample of the same quartet set, extrapolated to the full set
+             on seeded uniform samples of the same quartet set (the procedure of --impl reference)
 
---impl reference times that libcint CPU path alone (rank 0) on the same workload and metric.
+--impl reference times that libcint CPU path alone (rank 0) on the same workload and metric:
+each step is one seeded uniform sample of the quartet set (about 1.5 s of libcint work), and
+value = the samples' integrals / their libcint time.
 Multi-GPU: chunks are distributed over ranks by their flop estimate (strong scaling: the
 total work is the molecule's quartet set, no collective on the data path).
 """
@@ -62,6 +67,7 @@ SCHWARZ = 1e-12
 # (5e-11 selects 0.5% of the mol40 quartets and measures 4.6% slower: the FP64 pipe is not the bound)
 FP32_BUDGET = 0.0
 PRIM_BUDGET = 5e-11  # tuned form: bound on the skipped primitive terms of one block
+NORTH_STAR_FP32_BUDGET = 5e-11  # the north-star record: FP32 recurrences where their estimated error fits
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cint_cpu_bench")
 
@@ -79,7 +85,11 @@ def parse():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--form", default="tuned", choices=["tuned", "plain"])
     ap.add_argument("--no-error", action="store_true")
-    ap.add_argument("--error-chunks", type=int, default=4)
+    ap.add_argument("--error-chunks", type=int, default=2)
+    ap.add_argument("--libcint-per-class", type=int, default=2000,
+                    help="quartets per class in the error_vs_libcint sample")
+    ap.add_argument("--no-decomposition", action="store_true",
+                    help="skip the FP64-autotuned-shapes and north-star-form comparison sweeps")
     ap.add_argument("--fp32-budget", type=float, default=FP32_BUDGET)
     ap.add_argument("--no-autotune", action="store_true", help="tuned form without the launch-shape autotuner")
     ap.add_argument("--no-jk", action="store_true", help="skip the direct J/K build timing")
@@ -182,38 +192,37 @@ def run_libcint(mol, quartets, threads):
     return json.loads(r.stdout)
 
 
-def cpu_rate(mol, sampler, nq_total, nint_total, seconds, threads):
-    """libcint time per quartet on a seeded uniform sample, extrapolated to the full set."""
-    n = 2000
-    res = run_libcint(mol, sampler(n, 1), threads)
-    per_q = res["seconds"] / n
-    n = int(min(5_000_000, max(n, seconds / max(per_q, 1e-9))))
-    res = run_libcint(mol, sampler(n, 2), threads)
-    per_q = res["seconds"] / n
-    full_s = per_q * nq_total
-    return {"value": nint_total / full_s / 1e9, "unit": "Gint/s", "cores": int(res["threads"]),
-            "kind": "reference",
-            "sample": "%d quartets drawn uniformly (seeded) from the %d-quartet set, %.1f s of libcint "
-                      "int2e_sph with an optimizer, OpenMP dynamic; extrapolated by quartet count" %
-                      (n, nq_total, res["seconds"]),
-            "seconds": res["seconds"]}
+def libcint_steps(mol, sampler, steps, warmup, threads, target_s=1.5, seed0=1000):
+    """libcint on seeded uniform samples of a workload's tuple set: warmup + steps samples of
+    the same size (sized by a calibration run for about target_s seconds of libcint work each),
+    sample s drawn with seed seed0 + s.  The one CPU procedure of both --impl reference and the
+    cpu_baseline record.  value = integrals of the timed samples / their libcint seconds."""
+    cal = run_libcint(mol, sampler(4000, seed0 - 1), threads)
+    per_q = cal["seconds"] / 4000
+    n = int(min(8_000_000, max(20_000, target_s / max(per_q, 1e-9))))
+    secs, ints = [], []
+    for s_ in range(warmup + steps):
+        r = run_libcint(mol, sampler(n, seed0 + s_), threads)
+        if s_ >= warmup:
+            secs.append(r["seconds"])
+            ints.append(r["nintegrals"])
+            threads_used = int(r["threads"])
+    return {"value": sum(ints) / sum(secs) / 1e9, "unit": "Gint/s", "cores": threads_used, "kind": "reference",
+            "sample": "%d steps of %d tuples drawn uniformly (seeded) from the tuple set, libcint 6.1.3 with an "
+                      "optimizer, OpenMP dynamic over the tuples; value = sampled integrals / libcint seconds" %
+                      (steps, n),
+            "tuples_per_step": n, "seconds_per_step": secs, "step_ms_mean": statistics.mean(secs) * 1e3,
+            "step_ms_spread": [min(secs) * 1e3, max(secs) * 1e3], "seconds_per_tuple": sum(secs) / (n * len(secs))}
 
 
 # ------------------------------------------------------------------ reference arm
 def schwarz_pairs_libcint(mol):
     """Q_ij = sqrt(max |(ij|ij)|) for all pairs i >= j, with libcint on the CPU."""
-    from concurrent.futures import ThreadPoolExecutor
     from oracle import RefLibcint
-    ref = RefLibcint()
-    pairs = [(i, j) for i in range(mol.nbas) for j in range(i + 1)]
-
-    def one(p):
-        out, _ = ref.int2e((p[0], p[1], p[0], p[1]), mol)
-        return np.sqrt(np.abs(out).max())
-
-    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
-        q = np.array(list(ex.map(one, pairs, chunksize=256)))
-    return np.array(pairs, dtype=np.int32), q
+    ii, jj = np.tril_indices(mol.nbas)
+    pairs = np.stack([ii, jj], axis=1).astype(np.int32)
+    vals, offs, _ = RefLibcint().batch(np.concatenate([pairs, pairs], axis=1), mol)
+    return pairs, np.sqrt(np.maximum.reduceat(np.abs(vals), offs[:-1]))
 
 
 class UniqueQuartets:
@@ -245,6 +254,21 @@ class UniqueQuartets:
         return np.concatenate([self.pairs[i], self.pairs[j]], axis=1).astype(np.int32)
 
 
+METRIC = "int2e_sph Gint/s at <=1e-10 abs err"
+DF_METRIC = "int3c2e_sph + int2c2e_sph Gint/s, density fitting"
+
+
+def reference_line(args, metric, value, steps_rec, cfg):
+    """The --impl reference JSON line: the measured sample steps are the timed region."""
+    return {"metric": metric, "value": value, "unit": "Gint/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": steps_rec["step_ms_mean"], "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference", "config": cfg,
+            "cpu_baseline": {k: steps_rec[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "step_ms_spread": steps_rec["step_ms_spread"],
+            "e2e": {"value": value, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -257,27 +281,12 @@ def reference_arm(args):
     mol = fn()
     uq = UniqueQuartets(mol, SCHWARZ)
     threads = os.cpu_count() or 1
-    # per-step sample sized for ~target seconds
-    cal = run_libcint(mol, uq.sample(2000, 100), threads)
-    per_q = cal["seconds"] / 2000
-    nsamp = int(min(2_000_000, max(2000, 8.0 / max(per_q, 1e-9))))
-    times = []
-    for s in range(args.warmup + args.steps):
-        res = run_libcint(mol, uq.sample(nsamp, 1000 + s), threads)
-        if s >= args.warmup:
-            times.append(res["seconds"] / nsamp * uq.nquartets)  # extrapolated full-step time
-    t = statistics.mean(times)
-    value = uq.nintegrals / t / 1e9
-    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (libcint CPU reference)", "value": value,
-            "unit": "Gint/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": args.workload, "description": desc, "nquartets": uq.nquartets,
-                       "nintegrals": uq.nintegrals, "schwarz_cutoff": SCHWARZ},
-            "cpu_baseline": {"value": value, "unit": "Gint/s", "cores": threads, "kind": "reference",
-                             "sample": "%d seeded uniform quartets per step, extrapolated by quartet count" % nsamp},
-            "e2e": {"value": value, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    rec = libcint_steps(mol, uq.sample, args.steps, args.warmup, threads)
+    cfg = {"workload": args.workload, "description": desc, "form": "libcint 6.1.3 int2e_sph on the host cores",
+           "nquartets": uq.nquartets, "nintegrals": uq.nintegrals, "schwarz_cutoff": SCHWARZ,
+           "step": "one seeded uniform sample of %d quartets of the set" % rec["tuples_per_step"],
+           "extrapolated_full_sweep_ms": rec["seconds_per_tuple"] * uq.nquartets * 1e3}
+    print(json.dumps(reference_line(args, METRIC, rec["value"], rec, cfg)))
 
 
 def df_problem(name):
@@ -296,15 +305,15 @@ class DFTriples:
     >= cutoff) built on the host from libcint Schwarz factors, with uniform sampling."""
 
     def __init__(self, mol, norb, cutoff):
-        from concurrent.futures import ThreadPoolExecutor
         from oracle import RefLibcint
         ref = RefLibcint()
-        pairs = [(i, j) for i in range(norb) for j in range(i + 1)]
-        aux = list(range(norb, mol.nbas))
-        with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
-            q = np.array(list(ex.map(lambda p: np.sqrt(np.abs(ref.int2e((p[0], p[1], p[0], p[1]), mol)[0]).max()),
-                                     pairs, chunksize=256)))
-            qk = np.array(list(ex.map(lambda k: np.sqrt(np.abs(ref.int2c2e((k, k), mol)[0]).max()), aux)))
+        ii, jj = np.tril_indices(norb)
+        pairs = np.stack([ii, jj], axis=1).astype(np.int32)
+        aux = np.arange(norb, mol.nbas, dtype=np.int32)
+        v, o, _ = ref.batch(np.concatenate([pairs, pairs], axis=1), mol)
+        q = np.sqrt(np.maximum.reduceat(np.abs(v), o[:-1]))
+        v, o, _ = ref.batch(np.stack([aux, aux], axis=1), mol)
+        qk = np.sqrt(np.maximum.reduceat(np.abs(v), o[:-1]))
         order = np.argsort(-qk, kind="stable")
         self.aux, self.qk = np.array(aux)[order], qk[order]
         self.pairs = np.array(pairs, dtype=np.int32)
@@ -335,33 +344,32 @@ def df_reference_arm(args):
     mol, norb, aux_pairs, desc = df_problem(args.workload)
     tri = DFTriples(mol, norb, SCHWARZ)
     threads = os.cpu_count() or 1
+    sampler = df_sampler(tri, aux_pairs, mol)
+    rec = libcint_steps(mol, sampler, args.steps, args.warmup, threads)
+    cfg = {"workload": args.workload, "description": desc,
+           "form": "libcint 6.1.3 int3c2e_sph + int2c2e_sph on the host cores", "ntriples": tri.nquartets,
+           "nintegrals": tri.nintegrals + int(sampler.n2int), "schwarz_cutoff": SCHWARZ,
+           "step": "one seeded sample of %d tuples: (ab|k) triples and (k|l) pairs in proportion to their counts"
+                   % rec["tuples_per_step"]}
+    print(json.dumps(reference_line(args, DF_METRIC, rec["value"], rec, cfg)))
+
+
+def df_sampler(tri, aux_pairs, mol):
+    """Sampler over the DF step's tuples: (ab|k) triples of the sweep and (k|l) metric pairs,
+    mixed in proportion to their counts."""
     l = mol.bas[:, 1]
-    n2int = int(((2 * l[aux_pairs[:, 0]] + 1) * (2 * l[aux_pairs[:, 1]] + 1)).sum())
     two = np.stack([aux_pairs[:, 0], np.full(len(aux_pairs), -1), aux_pairs[:, 1], np.full(len(aux_pairs), -1)],
                    axis=1).astype(np.int32)
-    cal = run_libcint(mol, tri.sample(2000, 100), threads)
-    per_q = cal["seconds"] / 2000
-    nsamp = int(min(2_000_000, max(2000, 8.0 / max(per_q, 1e-9))))
-    rng = np.random.default_rng(7)
-    times = []
-    for s_ in range(args.warmup + args.steps):
-        r3 = run_libcint(mol, tri.sample(nsamp, 1000 + s_), threads)
-        r2 = run_libcint(mol, two[rng.choice(len(two), size=min(len(two), 20000), replace=False)], threads)
-        if s_ >= args.warmup:
-            times.append(r3["seconds"] / nsamp * tri.nquartets + r2["seconds"] / min(len(two), 20000) * len(two))
-    t = statistics.mean(times)
-    value = (tri.nintegrals + n2int) / t / 1e9
-    line = {"metric": "int3c2e_sph + int2c2e_sph Gint/s, density fitting (libcint CPU reference)", "value": value,
-            "unit": "Gint/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": args.workload, "description": desc, "ntriples": tri.nquartets,
-                       "nintegrals": tri.nintegrals + n2int, "schwarz_cutoff": SCHWARZ},
-            "cpu_baseline": {"value": value, "unit": "Gint/s", "cores": threads, "kind": "reference",
-                             "sample": "%d seeded uniform (ab|k) triples and 20000 (k|l) pairs per step, "
-                                       "extrapolated by count" % nsamp},
-            "e2e": {"value": value, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    frac2 = len(two) / (len(two) + tri.nquartets)
+
+    def sample(n, seed):
+        n2 = int(round(n * frac2))
+        rng = np.random.default_rng(seed + 7919)
+        parts = [tri.sample(n - n2, seed), two[rng.integers(0, len(two), size=n2)]]
+        return np.concatenate(parts)
+
+    sample.n2int = int(((2 * l[aux_pairs[:, 0]] + 1) * (2 * l[aux_pairs[:, 1]] + 1)).sum())
+    return sample
 
 
 # ------------------------------------------------------------------ our arm
@@ -384,15 +392,18 @@ def fp64_peak(cx, torch):
     return best
 
 
-def timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=False):
+def timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=False, steps=None, warmup=None):
     """Warm-up, then exactly args.steps timed passes of `plan` over the rank's chunks (one CUDA
     graph per pass unless --no-graph), L2 flushed between passes outside the events.  With
-    tune, the plan's launch shapes are autotuned first (each class on its largest segment)."""
-    return timed_multi(cx, torch, [(plan, mine)], args, stream, local, world, tune)
+    tune, the plan's launch shapes are autotuned first (each class on its largest segment).
+    steps / warmup override args.steps / args.warmup (the comparison sweeps run fewer)."""
+    return timed_multi(cx, torch, [(plan, mine)], args, stream, local, world, tune, steps, warmup)
 
 
-def timed_multi(cx, torch, items, args, stream, local, world, tune=False):
+def timed_multi(cx, torch, items, args, stream, local, world, tune=False, steps=None, warmup=None):
     """As timed_sweep for several plans run back to back in one step: items = [(plan, chunks)]."""
+    nsteps = args.steps if steps is None else steps
+    nwarm = args.warmup if warmup is None else warmup
     import torch.distributed as dist
     rings = [torch.empty(max(p.stats.max_chunk_doubles, 1), dtype=torch.float64, device="cuda") for p, _ in items]
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -427,7 +438,7 @@ def timed_multi(cx, torch, items, args, stream, local, world, tune=False):
                 for c in mine:
                     plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
 
-    for _ in range(args.warmup):
+    for _ in range(nwarm):
         step()
     torch.cuda.synchronize()
     clocks = Clocks(local)
@@ -438,7 +449,7 @@ def timed_multi(cx, torch, items, args, stream, local, world, tune=False):
     launches0 = cx.launch_count()
     t_wall = time.perf_counter()
     step_ms = []
-    for _ in range(args.steps):
+    for _ in range(nsteps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -452,8 +463,8 @@ def timed_multi(cx, torch, items, args, stream, local, world, tune=False):
     t_wall = time.perf_counter() - t_wall
     launches = cx.launch_count() - launches0
     clk = clocks.stop()
-    ms = max_over_ranks(sum(step_ms), device="cuda") / args.steps
-    return {"ms": ms, "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": rings[0],
+    ms = max_over_ranks(sum(step_ms), device="cuda") / nsteps
+    return {"ms": ms, "steps": nsteps, "step_ms_spread": [min(step_ms), max(step_ms)], "launches": launches, "clocks": clk, "wall": t_wall, "graph": use_graph, "ring": rings[0],
             "rings": rings, "tuning": tuning}
 
 
@@ -516,7 +527,7 @@ def jk_timing(cx, torch, plan, mol, stream, reps):
 
 
 def tuned_error(cx, torch, opt, plan, ring, stream, max_chunks):
-    """Max and RMS absolute difference between the mixed plan and an FP64 evaluation of the same
+    """Max and RMS absolute difference between the tuned plan and an FP64 evaluation of the same
     quartets (explicit FP64 plan over each checked chunk's quartet list)."""
     st = plan.stats
     chunks = list(range(st.nchunks))
@@ -536,8 +547,159 @@ def tuned_error(cx, torch, opt, plan, ring, stream, max_chunks):
         ss += float((d * d).sum())
         n += d.numel()
         ref_plan.close()
+        del ref
     return {"max_abs": mx, "rms_abs": (ss / max(n, 1)) ** 0.5, "integrals_checked": n,
             "chunks_checked": len(chunks), "reference": "the same quartets evaluated by the FP64 kernels"}
+
+
+def class_codes(quartets, lvals):
+    """Kernel class of each int2e quartet as an int: 100*(10 la + lb) + (10 lc + ld), the pairs
+    oriented larger l first and the pair of larger (la, lb) first (the class the kernels run)."""
+    l = lvals[quartets]
+    p1 = 10 * np.maximum(l[:, 0], l[:, 1]) + np.minimum(l[:, 0], l[:, 1])
+    p2 = 10 * np.maximum(l[:, 2], l[:, 3]) + np.minimum(l[:, 2], l[:, 3])
+    return 100 * np.maximum(p1, p2) + np.minimum(p1, p2)
+
+
+def code_label(code):
+    a, b = divmod(int(code), 100)
+    return "(%d%d|%d%d)" % (a // 10, a % 10, b // 10, b % 10)
+
+
+def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
+    """The plan's own output for a class-stratified sample of its quartets against libcint 6.1.3
+    built from the reference sources (oracle/_ref).  Every chunk is evaluated into `ring`; each
+    quartet of a class with T quartets in the sweep is kept with probability per_class / T (all of
+    them when T <= per_class), and its block is read back from the chunk's output.  Reports max
+    and RMS absolute error over the sampled integrals, the share within the parity rule
+    |d| <= 1e-12 or |d| <= 1e-10 |ref| (cintx-oracle two_electron_parity.rs:26-33) and the worst
+    class."""
+    from oracle import RefLibcint
+    rng = np.random.default_rng(seed)
+    st = plan.stats
+    lv = mol.bas[:, 1].astype(np.int64)
+    nsph = 2 * lv + 1
+    totals = {}
+    for c in range(st.nchunks):
+        cls, nq, _ = plan.segments(c)
+        for cl, n in zip(cls, nq):
+            code = 100 * (10 * int(cl[0]) + int(cl[1])) + 10 * int(cl[2]) + int(cl[3])
+            totals[code] = totals.get(code, 0) + int(n)
+    t0 = time.perf_counter()
+    tuples, got = [], []
+    for c in range(st.nchunks):
+        q = plan.chunk_quartets(c)
+        codes = class_codes(q, lv)
+        prob = np.array([min(1.0, per_class / totals.get(int(k), 1)) for k in range(10000)])
+        sel = np.where(rng.random(len(q)) < prob[codes])[0]
+        if not len(sel):
+            continue
+        sizes = np.prod(nsph[q], axis=1)
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        lens = sizes[sel]
+        starts = offs[sel]
+        idx = np.repeat(starts - np.concatenate([[0], np.cumsum(lens)[:-1]]), lens) + np.arange(int(lens.sum()))
+        plan.execute(ring.data_ptr(), chunk=c, stream=stream.cuda_stream)
+        stream.synchronize()
+        got.append(ring[torch.from_numpy(idx).to(ring.device)].cpu().numpy())
+        tuples.append(q[sel])
+    tuples = np.concatenate(tuples)
+    got = np.concatenate(got)
+    t1 = time.perf_counter()
+    ref, offs, _ = RefLibcint().batch(tuples, mol)
+    t2 = time.perf_counter()
+    d = np.abs(got - ref)
+    ok = (d <= 1e-12) | (d <= 1e-10 * np.abs(ref))
+    codes = class_codes(tuples, lv)
+    per = {}
+    blk = np.repeat(codes, np.diff(offs))
+    order = np.argsort(blk, kind="stable")
+    bs, ds = blk[order], d[order]
+    cuts = np.flatnonzero(np.diff(bs)) + 1
+    for part_b, part_d in zip(np.split(bs, cuts), np.split(ds, cuts)):
+        per[code_label(part_b[0])] = float(part_d.max())
+    worst = max(per.items(), key=lambda kv: kv[1])
+    return {"max_abs": float(d.max()), "rms_abs": float(np.sqrt(np.mean(d * d))), "integrals_checked": int(d.size),
+            "quartets_checked": int(len(tuples)), "classes_checked": len(per),
+            "classes_in_sweep": len(totals), "per_class_target": per_class,
+            "parity_rule_share": float(ok.mean()), "worst_class": {"class": worst[0], "max_abs": worst[1]},
+            "within_1e-10": bool(d.max() <= 1e-10),
+            "reference": "libcint 6.1.3 built from the reference sources (oracle/_ref), same quartets, CPU",
+            "seconds": {"sweep_and_gather": t1 - t0, "libcint": t2 - t1}}
+
+
+# DRAM bytes per quartet measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch / its quartets) for the classes that have been the dominant kernel, with the profile
+# summary each figure comes from.
+NCU_TRAFFIC_PER_QUARTET = {
+    "(31|30)": (215.2e6 / 151552, "profiles/eri4c_3130_sliced8_2pass_mol120_spdf.md"),
+}
+
+
+def roofline_record(per_class, peak64, st, ms_per_step):
+    top = max(per_class.items(), key=lambda kv: kv[1]["ms"])
+    d = top[1]
+    achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
+    prof_total = sum(v["ms"] for v in per_class.values())
+    alg_bytes = 8.0 * d["ints"] / d["launches"]
+    tr = NCU_TRAFFIC_PER_QUARTET.get(top[0])
+    traffic = tr[0] * d["quartets"] / d["launches"] if tr else None
+    return {"bound": "fp64", "kernel": "eri4c_kernel" + top[0], "achieved": achieved, "peak": peak64,
+            "unit": "TFLOP/s", "frac": achieved / peak64,
+            "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
+            "share_of_step": d["ms"] / prof_total,
+            "traffic": traffic, "algorithmic_bytes": alg_bytes,
+            "traffic_over_algorithmic": traffic / alg_bytes if traffic else None,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per quartet (%s) x the class's "
+                               "quartets per launch" % tr[1]) if tr else "no ncu capture of this class",
+            "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
+
+
+def learned_root_sample(cx, torch, opt, plan, mol, stream, n, seed):
+    """Learned Rys roots on a seeded uniform sample of the sweep's quartets (an explicit plan: its
+    root buffer holds every primitive quartet's roots, which the full sweep's 1e10 primitive
+    quartets would not fit): RysNet trained on the device for 1..7 roots, the sample evaluated
+    with learned roots and with table roots (same launch shapes), times and errors vs libcint."""
+    from oracle import RefLibcint
+    quart = plan.sample_quartets(n, seed)
+    quart = np.unique(quart, axis=0)
+    net = cx.RysNet(seed=0)
+    t0 = time.perf_counter()
+    net.train(nsamples=5_000_000, n_lo=1, n_hi=7, epochs=40, batch=16384, lr=3e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    p_tab = cx.Plan.shells(opt, cx.INT2E, quart)
+    p_lrn = cx.Plan.shells(opt, cx.INT2E, quart)
+    p_tab.use_tuned_shapes()
+    p_lrn.use_tuned_shapes()
+    fb, npq = p_lrn.use_learned_roots(net)
+    nint = p_lrn.stats.nintegrals
+    a = torch.empty(nint, dtype=torch.float64, device="cuda")
+    b = torch.empty_like(a)
+    ms = {}
+    for name, p, buf in (("learned", p_lrn, a), ("table", p_tab, b)):
+        p.execute(buf.data_ptr(), stream=stream.cuda_stream)
+        stream.synchronize()
+        times = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.execute(buf.data_ptr(), stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms[name] = statistics.median(times)
+    ref, _, _ = RefLibcint().batch(quart, mol)
+    got = a.cpu().numpy()
+    d = np.abs(got - ref)
+    p_tab.close()
+    p_lrn.close()
+    return {"quartets": int(len(quart)), "integrals": int(nint), "primitive_quartets": int(npq),
+            "fallback": int(fb), "fallback_rate": fb / max(npq, 1), "train_seconds": train_s,
+            "gint_s_learned": nint / (ms["learned"] * 1e-3) / 1e9, "gint_s_table": nint / (ms["table"] * 1e-3) / 1e9,
+            "learned_over_table": ms["table"] / ms["learned"],
+            "max_abs_vs_libcint": float(d.max()), "rms_abs_vs_libcint": float(np.sqrt(np.mean(d * d))),
+            "what": "seeded uniform sample of the sweep's quartets as an explicit plan; roots from the device-trained "
+                    "MLP (1..7 roots) refined in FP64 with table fallback, vs table roots in the same kernels"}
 
 
 def our_arm(args):
@@ -558,57 +720,128 @@ def our_arm(args):
     opt = cx.Optimizer(mol.atm, mol.bas, mol.env)
     tuned = args.form == "tuned"
 
-    def make_plan(o, tuned_form):
-        if tuned_form:
+    def make_plan(o, form, chunk_doubles):
+        if form == "tuned":
             return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=args.fp32_budget, prim_budget=args.prim_budget,
-                                          max_chunk_doubles=args.chunk_doubles)
-        return cx.Plan.screened(o, SCHWARZ, sph=True, max_chunk_doubles=args.chunk_doubles)
+                                          max_chunk_doubles=chunk_doubles)
+        if form == "fp64_tuned_shapes":
+            return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=0.0, prim_budget=0.0,
+                                          max_chunk_doubles=chunk_doubles)
+        if form == "north_star":
+            return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=NORTH_STAR_FP32_BUDGET,
+                                          prim_budget=args.prim_budget, max_chunk_doubles=chunk_doubles)
+        return cx.Plan.screened(o, SCHWARZ, sph=True, max_chunk_doubles=chunk_doubles)
 
-    plan = make_plan(opt, tuned)
+    def shard(p):
+        return chunks_of(assign_chunks([float(p.segments(c)[2].sum()) for c in range(p.stats.nchunks)], world), rank)
+
+    plan = make_plan(opt, "tuned" if tuned else "plain", args.chunk_doubles)
     st = plan.stats
     nchunks = st.nchunks
-    chunk_flops = [float(plan.segments(c)[2].sum()) for c in range(nchunks)]
-    mine = chunks_of(assign_chunks(chunk_flops, world), rank)
-    my_ints = sum(plan.chunk_size(c) for c in mine)
+    mine = shard(plan)
     stream = torch.cuda.Stream()  # a real stream handle: events and kernels share it
     torch.cuda.set_stream(stream)
 
     main_run = timed_sweep(cx, torch, plan, mine, args, stream, local, world, tune=tuned and not args.no_autotune)
     ms_per_step = main_run["ms"]
     value = st.nintegrals / (ms_per_step * 1e-3) / 1e9
-    plain = None
+    # comparison sweeps (fewer steps; every rank runs them in the same order)
+    extra = {}
     if tuned:
-        pplan = make_plan(opt, False)
-        pst = pplan.stats
-        pmine = chunks_of(assign_chunks([float(pplan.segments(c)[2].sum()) for c in range(pst.nchunks)], world), rank)
-        prun = timed_sweep(cx, torch, pplan, pmine, args, stream, local, world)
-        plain = {"value": pst.nintegrals / (prun["ms"] * 1e-3) / 1e9, "ms_per_step": prun["ms"]}
-        pplan.close()
-        del prun
+        forms = ["plain"] + ([] if args.no_decomposition else ["fp64_tuned_shapes", "north_star"])
+        for form in forms:
+            p = make_plan(opt, form, args.chunk_doubles)
+            if form != "plain" and not args.no_autotune:
+                p.use_tuned_shapes()
+            run = timed_sweep(cx, torch, p, shard(p), args, stream, local, world, steps=max(1, min(args.steps, 5)),
+                              warmup=2)
+            ps = p.stats
+            extra[form] = {"plan": p, "value": ps.nintegrals / (run["ms"] * 1e-3) / 1e9, "ms_per_step": run["ms"],
+                           "steps": run["steps"], "nquartets_fp32": ps.nquartets_fp32,
+                           "nprim_quartets": ps.nprim_quartets, "ring": run["ring"]}
+            del run
 
     per_class = class_profile(torch, plan, mine, main_run["ring"], stream)
     peak64 = fp64_peak(cx, torch)
-    top = max(per_class.items(), key=lambda kv: kv[1]["ms"]) if per_class else (None, None)
-    roof = None
-    if top[0] is not None:
-        d = top[1]
-        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
-        prof_total = sum(v["ms"] for v in per_class.values())
-        roof = {"bound": "fp64", "kernel": "eri4c_kernel" + top[0], "achieved": achieved, "peak": peak64,
-                "unit": "TFLOP/s", "frac": achieved / peak64,
-                "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "share_of_step": d["ms"] / prof_total, "traffic": None,
-                "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
-    err = None
+    roof = roofline_record(per_class, peak64, st, ms_per_step) if per_class else None
+    err = err_lib = None
+    ns_rec = None
     if tuned and rank == 0 and not args.no_error:
         err = tuned_error(cx, torch, opt, plan, main_run["ring"], stream, args.error_chunks)
+        if os.path.exists(REF_DRIVER):
+            err_lib = error_vs_libcint(torch, plan, mol, main_run["ring"], stream, args.libcint_per_class, 2027)
+            if "north_star" in extra:
+                e = extra["north_star"]
+                ns_rec = {"error_vs_libcint": error_vs_libcint(torch, e["plan"], mol, e["ring"], stream, 500, 2028)}
+                ns_rec["learned_roots_sample"] = learned_root_sample(cx, torch, opt, plan, mol, stream, 100_000, 77)
+    for e in extra.values():
+        e["plan"].close()
+        e.pop("plan")
+        e.pop("ring")
     jk = None
     if rank == 0 and world == 1 and not args.no_jk:
         jk = jk_timing(cx, torch, plan, mol, stream, min(args.steps, 5))
+
+    # end-to-end through the C ABI from host arrays, measured on every rank over its own chunks:
+    # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory;
+    # the step time is the max over ranks
+    e2e = None
+    if not args.no_e2e:
+        e2e_chunk = args.e2e_chunk_doubles
+        host = None
+        phases = {"optimizer": [], "plan": [], "execute_d2h": []}
+        h2d = d2h = 0
+        for s_ in range(1 + max(1, min(args.steps, 3))):
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env)
+            t1 = time.perf_counter()
+            p2 = make_plan(o2, "tuned" if tuned else "plain", e2e_chunk)
+            if tuned and not args.no_autotune:
+                p2.use_tuned_shapes()  # shapes autotuned once in this process (before the timed sweep)
+            t2 = time.perf_counter()
+            if host is None or host.size < 2 * p2.stats.max_chunk_doubles:  # two-slot page-locked host ring
+                # allocated in the untimed first iteration; later iterations reuse it
+                host = torch.empty(2 * max(p2.stats.max_chunk_doubles, 1), dtype=torch.float64,
+                                   pin_memory=True).numpy()
+            e2e_mine = shard(p2)
+            if world == 1:
+                p2.execute_host_ring(host)
+                mine_ints = p2.stats.nintegrals
+            else:
+                mine_ints = 0
+                for c in e2e_mine:
+                    p2.execute_host(host, chunk=c)
+                    mine_ints += p2.chunk_size(c)
+            t3 = time.perf_counter()
+            if s_ > 0:
+                phases["optimizer"].append(t1 - t0)
+                phases["plan"].append(t2 - t1)
+                phases["execute_d2h"].append(t3 - t2)
+            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + p2.stats.device_bytes
+            d2h = mine_ints * 8
+            p2.close()
+            o2.close()
+        te_local = sum(statistics.mean(v) for v in phases.values())
+        te = max_over_ranks(te_local, device="cuda")
+        h2d_all = max_over_ranks(h2d, device="cuda") * world  # every rank uploads the basis and its plan
+        d2h_all = st.nintegrals * 8
+        e2e = {"value": st.nintegrals / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d_all),
+               "d2h_bytes_per_step": int(d2h_all), "seconds_per_step": te,
+               "phases_s": {k: statistics.mean(v) for k, v in phases.items()},
+               "chunk_doubles": e2e_chunk, "ranks_timed": world,
+               "includes": "int2e_optimizer from host atm/bas/env (pair tables, Schwarz passes) + screened "
+                           "plan + evaluation + D2H of every integral (each rank its own chunks; a two-chunk "
+                           "page-locked host ring overlapping copies with the next chunk's kernels at N=1); "
+                           "max over ranks"}
     if rank != 0:
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()
+        plan.close()
+        opt.close()
         return
 
     hbm = None
@@ -621,8 +854,7 @@ def our_arm(args):
                                                          "launch shapes autotuned per class" if not args.no_autotune
                                                          else "default launch shapes")) if tuned else \
         "plain FP64 (default launch shapes, libcint screening only)"
-    line = {"metric": "int2e_sph Gint/s at <=1e-10 abs err (%s form)" % ("tuned" if tuned else "plain FP64"),
-            "value": value, "unit": "Gint/s",
+    line = {"metric": METRIC, "value": value, "unit": "Gint/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded molecule; no dataset)",
@@ -636,6 +868,7 @@ def our_arm(args):
             "quartets_per_s": st.nquartets / (ms_per_step * 1e-3),
             "gpu_launches": main_run["launches"],
             "clocks": main_run["clocks"], "wall_s_timed_region": main_run["wall"],
+            "step_ms_spread": main_run["step_ms_spread"],
             "roofline": roof,
             "output_write_gbs": st.nintegrals * 8 / (ms_per_step * 1e-3) / 1e9,
             "hbm_gbs_measured_peak": hbm,
@@ -647,71 +880,46 @@ def our_arm(args):
             "profiled_step_ms": sum(v["ms"] for v in per_class.values())}
     if main_run["tuning"] is not None:
         line["autotune"] = main_run["tuning"]
-    if plain is not None:
-        line["plain_fp64"] = plain
-        line["tuned_over_plain"] = value / plain["value"]
+    if "plain" in extra:
+        line["plain_fp64"] = extra["plain"]
+        line["tuned_over_plain"] = value / extra["plain"]["value"]
+    if "fp64_tuned_shapes" in extra:
+        pv = extra["plain"]["value"]
+        sv = extra["fp64_tuned_shapes"]["value"]
+        line["decomposition"] = {
+            "plain_fp64": pv, "fp64_autotuned_shapes": sv, "tuned": value,
+            "autotuner_factor": sv / pv, "primitive_screening_factor": value / sv,
+            "what": "plain = default shapes, libcint screening; fp64_autotuned_shapes = the tuned plan's launch shapes "
+                    "with no primitive screening and no FP32; tuned = this line's value (autotuned shapes + primitive "
+                    "Schwarz screening within %g per integral)" % args.prim_budget}
+    if "north_star" in extra:
+        e = extra["north_star"]
+        rec = {"value": e["value"], "ms_per_step": e["ms_per_step"], "steps": e["steps"],
+               "over_plain": e["value"] / extra["plain"]["value"],
+               "fp32_budget": NORTH_STAR_FP32_BUDGET, "nquartets_fp32": e["nquartets_fp32"],
+               "fp32_quartet_share": e["nquartets_fp32"] / max(st.nquartets, 1),
+               "form": "autotuned shapes + primitive Schwarz screening + FP32 recurrences where the estimated FP32 "
+                       "error is below the budget, table roots in the full sweep (learned roots measured on a sample: "
+                       "their per-primitive-quartet root buffer does not fit the full sweep)"}
+        if ns_rec:
+            rec.update(ns_rec)
+            lr = ns_rec["learned_roots_sample"]["learned_over_table"]
+            rec["with_learned_roots_over_plain_estimate"] = rec["over_plain"] * lr
+            rec["meets_3x_at_1e-10"] = bool(rec["with_learned_roots_over_plain_estimate"] >= 3.0 and
+                                            ns_rec["error_vs_libcint"]["max_abs"] <= 1e-10)
+        line["north_star_form"] = rec
     if err is not None:
         line["error_vs_fp64"] = err
+    if err_lib is not None:
+        line["error_vs_libcint"] = err_lib
     if jk is not None:
         line["jk_build"] = jk
-
-    # end-to-end through the C ABI from host arrays (rank 0 measures its own shard when N > 1):
-    # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory
-    if not args.no_e2e:
-        e2e_chunk = args.e2e_chunk_doubles
-
-        def e2e_plan(o):
-            if tuned:
-                return cx.Plan.screened_mixed(o, SCHWARZ, fp32_budget=args.fp32_budget, prim_budget=args.prim_budget,
-                                              max_chunk_doubles=e2e_chunk)
-            return cx.Plan.screened(o, SCHWARZ, sph=True, max_chunk_doubles=e2e_chunk)
-
-        host = None
-        phases = {"optimizer": [], "plan": [], "execute_d2h": []}
-        h2d = d2h = 0
-        for s in range(1 + max(1, min(args.steps, 3))):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env)
-            t1 = time.perf_counter()
-            p2 = e2e_plan(o2)
-            if tuned and not args.no_autotune:
-                p2.use_tuned_shapes()  # shapes autotuned once in this process (before the timed sweep)
-            t2 = time.perf_counter()
-            if host is None or host.size < 2 * p2.stats.max_chunk_doubles:  # two-slot page-locked host ring
-                # allocated in the untimed first iteration; later iterations reuse it
-                host = torch.empty(2 * max(p2.stats.max_chunk_doubles, 1), dtype=torch.float64,
-                                   pin_memory=True).numpy()
-            if world == 1:
-                p2.execute_host_ring(host)
-            else:
-                e2e_mine = chunks_of(assign_chunks([float(p2.segments(c)[2].sum()) for c in range(p2.stats.nchunks)],
-                                                   world), rank)
-                off = 0
-                for c in e2e_mine:
-                    p2.execute_host(host, chunk=c)
-                    off += p2.chunk_size(c)
-            t3 = time.perf_counter()
-            if s > 0:
-                phases["optimizer"].append(t1 - t0)
-                phases["plan"].append(t2 - t1)
-                phases["execute_d2h"].append(t3 - t2)
-            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + p2.stats.device_bytes
-            d2h = (st.nintegrals if world == 1 else off) * 8
-            p2.close()
-            o2.close()
-        te = sum(statistics.mean(v) for v in phases.values())
-        line["e2e"] = {"value": st.nintegrals / te / 1e9 if world == 1 else d2h / 8 / te / 1e9 * world,
-                       "unit": "Gint/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                       "seconds_per_step": te,
-                       "phases_s": {k: statistics.mean(v) for k, v in phases.items()},
-                       "chunk_doubles": e2e_chunk,
-                       "includes": "int2e_optimizer from host atm/bas/env (pair tables, Schwarz passes) + screened "
-                                   "plan + evaluation + D2H of every integral through a two-chunk page-locked "
-                                   "host ring (copies overlapped with the next chunk's kernels)"}
+    if e2e is not None:
+        line["e2e"] = e2e
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
-        line["cpu_baseline"] = cpu_rate(mol, lambda n, seed: plan.sample_quartets(n, seed), st.nquartets,
-                                        st.nintegrals, args.cpu_seconds, os.cpu_count() or 1)
+        uq = UniqueQuartets(mol, SCHWARZ)
+        cb = libcint_steps(mol, uq.sample, 3, 1, os.cpu_count() or 1)
+        line["cpu_baseline"] = cb
     elif world == 1 and not args.no_cpu:
         line["cpu_baseline"] = None
     print(json.dumps(line))
@@ -774,22 +982,47 @@ def df_arm(args):
         q2.close()
     per_class = class_profile(torch, p3, mine3, run["rings"][0], stream)
     peak64 = fp64_peak(cx, torch)
-    roof = None
-    if per_class:
-        top = max(per_class.items(), key=lambda kv: kv[1]["ms"])
-        d = top[1]
-        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
-        roof = {"bound": "fp64", "kernel": "eri4c_kernel" + top[0], "achieved": achieved, "peak": peak64,
-                "unit": "TFLOP/s", "frac": achieved / peak64,
-                "peak_source": "FP64 FMA probe kernel on this GPU, this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "share_of_step": d["ms"] / sum(v["ms"] for v in per_class.values()), "traffic": None}
+    from types import SimpleNamespace
+    roof = roofline_record(per_class, peak64, SimpleNamespace(flops=s3.flops + s2.flops), run["ms"]) \
+        if per_class else None
+    e2e = None
+    if not args.no_e2e:
+        # end to end from host arrays on every rank: optimizer, both plans, evaluation of the rank's
+        # 3-centre chunks (rank 0 also the 2-centre metric) and D2H of each into a page-locked host
+        # buffer (one chunk at a time: the 3-centre output exceeds host memory); max over ranks
+        host = torch.empty(max(s3.max_chunk_doubles, s2.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
+        times = []
+        for s_ in range(2):
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
+            e3, e2 = make(o2)
+            if tuned and not args.no_autotune:
+                e3.use_tuned_shapes()
+                e2.use_tuned_shapes()
+            for c in chunks_of(assign_chunks([float(e3.segments(c)[2].sum()) for c in range(e3.stats.nchunks)],
+                                             world), rank):
+                e3.execute_host(host, chunk=c)
+            if rank == 0:
+                e2.execute_host(host)
+            times.append(time.perf_counter() - t0)
+            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + e3.stats.device_bytes
+            e3.close()
+            e2.close()
+            o2.close()
+        te = max_over_ranks(times[-1], device="cuda")
+        e2e = {"value": nint / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d) * world,
+               "d2h_bytes_per_step": int(nint * 8), "seconds_per_step": te, "ranks_timed": world,
+               "includes": "optimizer from host atm/bas/env, both plans (Schwarz passes), evaluation and "
+                           "D2H of every integral, chunk by chunk, each rank its own chunks; max over ranks"}
     if rank != 0:
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()
         return
-    line = {"metric": "int3c2e_sph + int2c2e_sph Gint/s, density fitting (%s form)" % ("tuned" if tuned else "plain"),
-            "value": value, "unit": "Gint/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    line = {"metric": DF_METRIC, "value": value, "unit": "Gint/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": run["ms"], "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded molecule and auxiliary basis; no dataset)",
             "config": {"workload": args.workload, "description": desc, "ntriples": s3.nquartets,
@@ -811,43 +1044,11 @@ def df_arm(args):
         line["tuned_over_plain"] = value / plain["value"]
     if err is not None:
         line["error_vs_default_shapes"] = err
-    if not args.no_e2e:
-        # end to end from host arrays: optimizer, both plans, evaluation and D2H of every chunk into
-        # a page-locked host buffer (one chunk at a time: the 3-centre output exceeds host memory)
-        host = torch.empty(max(s3.max_chunk_doubles, s2.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
-        times = []
-        for s_ in range(2):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            o2 = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
-            e3, e2 = make(o2)
-            if tuned and not args.no_autotune:
-                e3.use_tuned_shapes()
-                e2.use_tuned_shapes()
-            for c in range(e3.stats.nchunks):
-                e3.execute_host(host, chunk=c)
-            e2.execute_host(host)
-            times.append(time.perf_counter() - t0)
-            h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + e3.stats.device_bytes
-            e3.close()
-            e2.close()
-            o2.close()
-        te = times[-1]
-        line["e2e"] = {"value": nint / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d),
-                       "d2h_bytes_per_step": int(nint * 8), "seconds_per_step": te,
-                       "includes": "optimizer from host atm/bas/env, both plans (Schwarz passes), evaluation and "
-                                   "D2H of every integral, chunk by chunk"}
+    if e2e is not None:
+        line["e2e"] = e2e
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
-        n3 = min(200000, s3.nquartets)
-        r3 = run_libcint(mol, p3.sample_quartets(n3, 1), os.cpu_count() or 1)
-        n2 = min(20000, s2.nquartets)
-        r2 = run_libcint(mol, p2.sample_quartets(n2, 2), os.cpu_count() or 1)
-        t_full = r3["seconds"] / n3 * s3.nquartets + r2["seconds"] / n2 * s2.nquartets
-        line["cpu_baseline"] = {"value": nint / t_full / 1e9, "unit": "Gint/s", "cores": int(r3["threads"]),
-                                "kind": "reference",
-                                "sample": "%d (ab|k) triples and %d (k|l) pairs drawn uniformly from the plans, "
-                                          "libcint int3c2e_sph/int2c2e_sph with optimizers, OpenMP dynamic; "
-                                          "extrapolated by count" % (n3, n2)}
+        tri = DFTriples(mol, norb, SCHWARZ)
+        line["cpu_baseline"] = libcint_steps(mol, df_sampler(tri, aux_pairs, mol), 3, 1, os.cpu_count() or 1)
     print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -102,6 +102,17 @@ int compute_prim_schwarz(Opt* o);
 // (unit pairs are built for every shell).
 int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env, int npair_shells = -1);
 
+// Offsets (doubles from the start of the payload) of each order's polynomial block and
+// asymptotic constants in the device layout of the Rys table, and its interval counts.
+struct RysTableOffsets {
+  size_t poly[CINTX_NRMAX + 1];
+  size_t asym[CINTX_NRMAX + 1];
+  int xmax[CINTX_NRMAX + 1];
+};
+// The embedded table checked against the compiled layout and transposed to the device layout
+// (rys_table.cu).  Returns 0 on success.
+int rys_table_image(std::vector<double>& payload, RysTableOffsets& offs);
+
 // Per-device constants (Rys table) and per-thread scratch.
 struct DeviceState {
   int dev = -1;

@@ -27,12 +27,9 @@
 #include "../../include/cintx_cuda.h"
 #include "host_internal.h"
 
-extern "C" const unsigned char cintx_rys_table_bin[];
-extern "C" const unsigned char cintx_rys_table_bin_end[];
-
 namespace {
 
-constexpr size_t kRysTableDoubles = 87040;  // >= doubles in rys_table.bin after its header
+constexpr size_t kRysTableDoubles = 87040;  // >= doubles in the device layout of the Rys table
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CINTX_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) double g_noalloc_rys[kRysTableDoubles];
@@ -47,8 +44,8 @@ std::mutex g_mu;
 NoallocDevice g_dev[64];
 
 // Once per device, with that device current: resolve the arrays' device addresses and copy the
-// root table (coefficients reordered to [interval][function][degree], the layout the kernels
-// read) into g_noalloc_rys.
+// root table, checked and laid out by rys_table_image exactly as the allocating path uploads it,
+// into g_noalloc_rys.
 int setup_device(int dev, NoallocDevice** out) {
   std::lock_guard<std::mutex> lk(g_mu);
   NoallocDevice& d = g_dev[dev];
@@ -65,40 +62,21 @@ int setup_device(int dev, NoallocDevice** out) {
                      std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
     return CINTX_STATUS_EXECUTION_FAILED;
   }
-  const unsigned char* p = cintx_rys_table_bin;
-  const size_t nbytes = (size_t)(cintx_rys_table_bin_end - cintx_rys_table_bin);
-  int64_t hdr[16];
-  memcpy(hdr, p, sizeof(hdr));
-  const int nmax = (int)hdr[0], deg = (int)hdr[1], nc = deg + 1;
-  const size_t ndbl = (nbytes - sizeof(hdr)) / sizeof(double);
-  if (nmax < CINTX_NRMAX || deg != CINTX_RYS_DEG || ndbl > kRysTableDoubles) {
-    cintx::set_error(CINTX_STATUS_EXECUTION_FAILED, "Rys table does not fit its static device array");
+  std::vector<double> host;
+  cintx::RysTableOffsets offs;
+  if (cintx::rys_table_image(host, offs) || host.size() > kRysTableDoubles) {
+    cintx::set_error(CINTX_STATUS_EXECUTION_FAILED, "Rys table does not match the layout of its static device array");
     return CINTX_STATUS_EXECUTION_FAILED;
   }
-  std::vector<double> host(ndbl);
-  memcpy(host.data(), p + sizeof(hdr), ndbl * sizeof(double));
   RysTable t;
   memset(&t, 0, sizeof(t));
   const double* base = (const double*)table;
-  size_t o = 0;
-  std::vector<double> tmp;
-  for (int n = 1; n <= nmax; ++n) {
-    const int nf = 2 * n, xmax = (int)hdr[1 + n];
-    if (n <= CINTX_NRMAX) {
-      t.poly[n] = base + o;
-      t.xmax[n] = xmax;
-    }
-    for (int i = 0; i < xmax; ++i, o += (size_t)nf * nc) {
-      tmp.assign(host.begin() + o, host.begin() + o + (size_t)nf * nc);
-      for (int k = 0; k < nc; ++k)
-        for (int f = 0; f < nf; ++f) host[o + (size_t)f * nc + k] = tmp[(size_t)k * nf + f];
-    }
+  for (int n = 1; n <= CINTX_NRMAX; ++n) {
+    t.poly[n] = base + offs.poly[n];
+    t.asym[n] = base + offs.asym[n];
+    t.xmax[n] = offs.xmax[n];
   }
-  for (int n = 1; n <= nmax; ++n) {
-    if (n <= CINTX_NRMAX) t.asym[n] = base + o;
-    o += 2 * n;
-  }
-  e = cudaMemcpy(table, host.data(), ndbl * sizeof(double), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(table, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cintx::set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("Rys table copy failed: ") + cudaGetErrorString(e));
     return CINTX_STATUS_EXECUTION_FAILED;
@@ -249,8 +227,13 @@ extern "C" int cintx_int2e_noalloc(double* out_dev, const int* shls, int64_t n, 
     r0 += kv.second.size();
   }
   cudaStream_t s = (cudaStream_t)stream;
-  // pageable source: the call returns once the image has been consumed, so it may go out of scope
-  cudaError_t e = cudaMemcpyAsync(nd->scratch, image.data(), total, cudaMemcpyHostToDevice, s);
+  // The image is host memory of this call.  Earlier work on the stream (a previous call's kernels
+  // still reading the shared array) must finish before the array is overwritten, and the copy
+  // must have read the image before the call returns: wait for the stream, copy on it, wait for
+  // the copy.  CUDA reports a failure of any step as an error, which the call returns.
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(nd->scratch, image.data(), total, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("scratch upload failed: ") + cudaGetErrorString(e));
     return CINTX_STATUS_EXECUTION_FAILED;

@@ -301,11 +301,12 @@ CINTX_API void cintx_plan_destroy(CintxPlan *plan);
  * (looks up the arrays' device addresses and copies the root table, synchronously); make that
  * first call before any stream capture.  A call whose screened pairs and quartet records exceed
  * the array returns CINTX_STATUS_MEMORY_LIMIT_EXCEEDED (split the list); classes with two or
- * more g shells return CINTX_STATUS_UNSUPPORTED_API.  Work is queued on `stream` (used as
- * given) and the function returns once its inputs have been copied.  Every call reuses the
- * same array and rewrites all of it that it reads, so nothing needs clearing between calls, but
- * calls whose work overlaps on the GPU (other streams, other host threads) race on it:
- * serialise them. */
+ * more g shells return CINTX_STATUS_UNSUPPORTED_API.  Each call builds its tables in host
+ * memory that lives only for the call: it waits for earlier work on `stream` (used as given),
+ * copies the tables into the array and waits for that copy, then queues its kernels on `stream`
+ * and returns without waiting for them.  Every call reuses the same array and rewrites all of it
+ * that it reads, so nothing needs clearing between calls, but calls whose work overlaps on the
+ * GPU (other streams, other host threads) race on it: serialise them. */
 CINTX_API int cintx_int2e_noalloc(double *out_dev, const int *shls, int64_t n, int sph, const int *atm,
                                   int natm, const int *bas, int nbas, const double *env, void *stream);
 

@@ -21,12 +21,19 @@ _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
 
+def reference_root() -> str:
+    """Root of the reference tree whose libcint sources oracle/Makefile compiles: the
+    CINTX_REFERENCE_ROOT environment variable, else the Makefile's default mount."""
+    return os.environ.get("CINTX_REFERENCE_ROOT", "/root/reference")
+
+
 def build(ref: bool = True) -> None:
     """Compile the restatement (and libcint from the reference sources when present)."""
     targets = ["liboracle_cint.so"]
-    if ref and os.path.isdir("/root/reference/libcint-master"):
+    root = reference_root()
+    if ref and os.path.isdir(os.path.join(root, "libcint-master")):
         targets += ["ref"]
-    subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", "CINTX_REFERENCE_ROOT=" + root] + targets, check=True)
 
 
 def _ip(a: np.ndarray):
@@ -174,6 +181,39 @@ class RefLibcint(_Base):
 
     def int2c2e(self, shls, mol, sph=True):
         return self.call("int2c2e_sph" if sph else "int2c2e_cart", shls, mol, sph)
+
+    _batch_lib = None
+
+    def batch(self, tuples, mol, sph=True, nthreads=0):
+        """Blocks of every tuple (rows of 4, 3 or 2 shell ids: int2e, int3c2e, int2c2e) from
+        libcint, concatenated in order (_ref/libcint_batch.so, OpenMP over the tuples).
+        Returns (values, offsets[n+1], return values)."""
+        if RefLibcint._batch_lib is None:
+            L = ctypes.CDLL(os.path.join(HERE, "_ref", "libcint_batch.so"))
+            L.ref_batch.argtypes = [ctypes.c_int, ctypes.c_int, _c_dbl_p, ctypes.POINTER(ctypes.c_longlong),
+                                    _c_int_p, ctypes.c_longlong, _c_int_p, ctypes.c_int, _c_int_p, ctypes.c_int,
+                                    _c_dbl_p, ctypes.c_int, _c_int_p]
+            L.ref_batch.restype = ctypes.c_int
+            RefLibcint._batch_lib = L
+        t = np.ascontiguousarray(tuples, dtype=np.int32)
+        fam = t.shape[1]
+        atm, bas, env = self._mol(mol)
+        l = bas[:, 1].astype(np.int64)
+        nc = bas[:, 3].astype(np.int64)
+        per = (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
+        sizes = np.prod(per[t], axis=1) if len(t) else np.zeros(0, dtype=np.int64)
+        offs = np.zeros(len(t) + 1, dtype=np.int64)
+        offs[1:] = np.cumsum(sizes)
+        out = np.zeros(int(offs[-1]))
+        rets = np.zeros(len(t), dtype=np.int32)
+        if len(t):
+            rc = RefLibcint._batch_lib.ref_batch(fam, int(sph), _dp(out),
+                                                 offs.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _ip(t),
+                                                 len(t), _ip(atm), atm.shape[0], _ip(bas), bas.shape[0], _dp(env),
+                                                 int(nthreads), _ip(rets))
+            if rc:
+                raise MemoryError("ref_batch: cache allocation failed")
+        return out, offs, rets
 
 
 def block_len(mol, shls, sph=True) -> int:

@@ -7,6 +7,9 @@
                      reference sources (oracle/_ref/libcint.so, built by oracle/Makefile) for
                      seeded samples of shell tuples of the synthetic molecules, plus a small
                      generally-contracted basis (nctr = 2) and dims / expcutoff variants.
+  libcint_mol120f.npz  libcint blocks of 50 quartets from every f-containing angular-momentum
+                     class of the 120-atom molecule's Schwarz-screened quartet set, each quartet
+                     in a random one of its 8 index orders.
 
 Run from the repository root: python tests/golden/make_golden.py   (needs oracle/_ref)
 """
@@ -148,9 +151,86 @@ def make_integrals():
     np.savez_compressed(os.path.join(HERE, "libcint_ctr2.npz"), **d)
 
 
+def schwarz_pairs(ref, mol):
+    """Every shell pair i >= j with q_ij = sqrt(max |(ij|ij)|) from libcint."""
+    ii, jj = np.tril_indices(mol.nbas)
+    pairs = np.stack([ii, jj], axis=1).astype(np.int32)
+    vals, offs, _ = ref.batch(np.concatenate([pairs, pairs], axis=1), mol)
+    q = np.sqrt(np.maximum.reduceat(np.abs(vals), offs[:-1]))
+    return pairs, q
+
+
+def class_stratified_quartets(ref, mol, cutoff, per_class, seed, need_l=3):
+    """Seeded sample of per_class quartets (or all, if fewer) from every angular-momentum class
+    that contains a shell of l == need_l, drawn uniformly within the class from the 8-fold-unique
+    quartets whose Schwarz bound q_ij q_kl reaches cutoff; each quartet is then put in a random
+    one of its 8 equivalent index orders.  Returns {class label: tuples}."""
+    rng = np.random.default_rng(seed)
+    pairs, q = schwarz_pairs(ref, mol)
+    order = np.argsort(-q, kind="stable")
+    pairs, q = pairs[order], q[order]
+    keep = q * q.max() >= cutoff
+    pairs, q = pairs[keep], q[keep]
+    # partners of pair position i: positions j <= i (q_j >= q_i) with q_i q_j >= cutoff
+    count = np.minimum(np.arange(len(q)) + 1, np.searchsorted(-q, -(cutoff / q), side="right"))
+    l = mol.bas[:, 1]
+    la, lb = l[pairs[:, 0]], l[pairs[:, 1]]
+    pc = 10 * np.maximum(la, lb) + np.minimum(la, lb)
+    idx = {c: np.where(pc == c)[0] for c in np.unique(pc)}
+    out = {}
+    for A in sorted(idx):
+        for B in sorted(idx):
+            if B > A or (A // 10 != need_l and A % 10 != need_l and B // 10 != need_l and B % 10 != need_l):
+                continue
+            # (i, j) with {pc_i, pc_j} = {A, B}: i of class X, partner j < count[i] of class Y
+            cand_i, cand_w, cand_y = [], [], []
+            for X, Y in ((A, B), (B, A)) if A != B else ((A, B),):
+                ix = idx[X]
+                w = np.searchsorted(idx[Y], count[ix])
+                cand_i.append(ix)
+                cand_w.append(w)
+                cand_y.append(np.full(len(ix), Y))
+            ci, cw, cy = np.concatenate(cand_i), np.concatenate(cand_w), np.concatenate(cand_y)
+            total = int(cw.sum())
+            if total == 0:
+                continue
+            n = min(per_class, total)
+            pick = rng.choice(len(ci), size=n, p=cw / total)
+            rows = []
+            for k in pick:
+                j = idx[cy[k]][rng.integers(0, cw[k])]
+                a, b = pairs[ci[k]]
+                c, d = pairs[j]
+                if rng.random() < 0.5:
+                    a, b = b, a
+                if rng.random() < 0.5:
+                    c, d = d, c
+                if rng.random() < 0.5:
+                    a, b, c, d = c, d, a, b
+                rows.append((a, b, c, d))
+            out["(%d%d|%d%d)" % (A // 10, A % 10, B // 10, B % 10)] = np.array(rows, dtype=np.int32)
+    return out
+
+
+def make_mol120():
+    """libcint blocks for a class-stratified sample of the 120-atom f-shell molecule's Schwarz-
+    screened (1e-12) quartet set: 50 quartets of every class containing an f shell."""
+    ref = RefLibcint()
+    mol = M.mol120()
+    per = class_stratified_quartets(ref, mol, 1e-12, 50, 120)
+    labels = sorted(per)
+    tuples = np.concatenate([per[k] for k in labels])
+    cls = np.concatenate([np.full(len(per[k]), i, dtype=np.int32) for i, k in enumerate(labels)])
+    vals, offs, rets = ref.batch(tuples, mol)
+    np.savez_compressed(os.path.join(HERE, "libcint_mol120f.npz"), int2e_sph_tuples=tuples,
+                        int2e_sph_offsets=offs, int2e_sph_values=vals, int2e_sph_ret=rets,
+                        class_index=cls, class_labels=np.array(labels))
+
+
 if __name__ == "__main__":
     make_roots()
     make_integrals()
+    make_mol120()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -265,6 +265,44 @@ def test_every_launch_shape_gives_the_same_integrals(cx):
         plan.close()
 
 
+def test_f_shell_classes_match_libcint_in_every_shape(cx):
+    """50 quartets of every f-containing class of the 120-atom molecule (the classes of the
+    headline sweep, in random index orders) against libcint at the parity rule, in each launch
+    shape the autotuner can pick (variants 0..9) and in the shapes it picks for them."""
+    mol = M.mol120()
+    g = np.load(os.path.join(GOLD, "libcint_mol120f.npz"))
+    tup, ref = g["int2e_sph_tuples"], g["int2e_sph_values"]
+    cls, labels, offs = g["class_index"], g["class_labels"], g["int2e_sph_offsets"]
+    import torch
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.shells(opt, cx.INT2E, tup, sph=True)
+        assert np.array_equal(plan.offsets, offs[:-1])
+        n = plan.stats.nintegrals
+        buf = torch.empty(n, dtype=torch.float64, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        lanes = set()
+        for v in list(range(10)) + ["tuned"]:
+            if v == "tuned":
+                plan.autotune(buf.data_ptr(), chunk=0, stream=s, reps=1)
+            else:
+                assert plan.set_shape(v) >= 0
+            lanes.add(tuple(plan.segment_lanes(0)))
+            buf.fill_(float("nan"))
+            plan.execute(buf.data_ptr(), stream=s)
+            torch.cuda.synchronize()
+            got = buf.cpu().numpy()
+            for c, lab in enumerate(labels):
+                for q in np.where(cls == c)[0]:
+                    a, b = got[offs[q]:offs[q + 1]], ref[offs[q]:offs[q + 1]]
+                    assert close(a, b), (v, lab, tup[q], np.abs(a - b).max())
+        assert len(lanes) > 1  # the variants did change the launch shapes
+        plan.close()
+    # the per-call libcint-signature path on a subset of the same blocks
+    for q in range(0, len(tup), 9):
+        out, ret = cx.int2e_sph(tup[q], mol.atm, mol.bas, mol.env)
+        assert ret == g["int2e_sph_ret"][q] and close(out, ref[offs[q]:offs[q + 1]]), tup[q]
+
+
 def test_graph_replay_matches_direct_execution(cx):
     mol = M.mol40()
     import torch

@@ -78,6 +78,20 @@ def test_oracle_vs_golden_general_contraction(orc):
     _check_family(orc, mol, g, "int3c2e_sph", lambda t, m: orc.int3c2e(t, m, True))
 
 
+def test_oracle_vs_golden_f_shell_classes(orc):
+    """The restatement on 50 quartets of every f-containing class of the 120-atom molecule
+    (libcint blocks of the Schwarz-screened set, random index orders)."""
+    mol = M.mol120()
+    g = gold("libcint_mol120f.npz")
+    tup = g["int2e_sph_tuples"]
+    offs = g["int2e_sph_offsets"]
+    out, o2 = orc.int2e_batch(tup, mol, True)
+    assert np.array_equal(o2, offs[:-1])
+    assert close(out, g["int2e_sph_values"]), np.abs(out - g["int2e_sph_values"]).max()
+    labels = g["class_labels"]
+    assert len(labels) == 34 and np.bincount(g["class_index"]).min() == 50
+
+
 def test_oracle_c2s_is_orthonormal_on_sphere(orc):
     # rows of the l >= 2 transforms, applied to cartesian monomials, give real spherical
     # harmonics; check via the known d(xy) coefficient sqrt(15/(4 pi)) and row count

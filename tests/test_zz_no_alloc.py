@@ -51,12 +51,25 @@ def test_noalloc_matches_plan_on_two_calls_in_a_row():
     for mol, quartets, sph in cases:
         ref = _reference(cx, mol, quartets.astype(np.int32), sph)
         out = torch.full((ref.size,), float("nan"), dtype=torch.float64, device="cuda")
+        stream.wait_stream(torch.cuda.current_stream())  # the NaN fill lands before the call's kernels
         rc = _noalloc(cx.lib, out.data_ptr(), quartets, mol, sph, stream.cuda_stream)
         assert rc == 0, cx.last_error()
         stream.synchronize()
         got = out.cpu().numpy()
         assert np.isfinite(got).all()
         assert close(got, ref), np.abs(got - ref).max()
+    # the entry point's promise: a call takes no device memory (the same work again, after the
+    # kernels it launches were loaded by the call above, leaves the device's free bytes unchanged)
+    mol, quartets, sph = cases[-1]
+    out.fill_(float("nan"))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    rc = _noalloc(cx.lib, out.data_ptr(), quartets, mol, sph, stream.cuda_stream)
+    stream.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert rc == 0, cx.last_error()
+    assert free1 == free0, (free0, free1)
+    assert close(out.cpu().numpy(), ref)
 
 
 def test_noalloc_rejects_calls_beyond_its_scratch():
