@@ -44,6 +44,7 @@ __host__ __device__ constexpr int binom(int n, int k) {
   return r;
 }
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
 
 // Threads per quartet: smallest power of two keeping <= 24 accumulators per lane, capped by
 // the tuple count and by 256.
@@ -154,7 +155,50 @@ struct EriShape {
   static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
   static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
   static constexpr int SMEM_BYTES = Q * B_GROUP + TABLE_DOUBLES * 8;
+  static constexpr bool IS_SLICE = SLICE;
+  static constexpr int NPASS = PASSES;
 };
+
+// Index bounds of a launch shape.  Every shared-memory, scratch, barrier and per-thread index
+// eri4c_kernel forms is a function of the shape's constants and of threadIdx.x < BLOCK, so these
+// conditions bound all of them; the kernel static_asserts the result for every compiled shape.
+// Returns 0, or the number of the first condition that fails.
+template <class SH>
+__host__ __device__ constexpr int shape_violation() {
+  // 1: S is a power of two in [1, 256]; a sliced shape splits its S slices over PASSES passes
+  if (SH::S < 1 || SH::S > 256 || (SH::S & (SH::S - 1)) != 0) return 1;
+  if (SH::IS_SLICE ? (SH::S % SH::NPASS != 0 || SH::LANES * SH::NPASS != SH::S) : SH::LANES != SH::S) return 1;
+  // 2: the block is a whole number of quartet groups (group = threadIdx.x / S, or for sliced
+  //    shapes set * 32 + lane with 32 * LANES threads per set), so group < Q
+  if (SH::BLOCK > 1024 || SH::BLOCK % (SH::IS_SLICE ? 32 * SH::LANES : SH::S) != 0) return 2;
+  if (SH::Q * SH::LANES != SH::BLOCK) return 2;
+  // 3: every (j,k,l) tuple has an owner: lane + S*k over k < TPT covers [0, NTUP)
+  if (SH::TPT * SH::S < SH::NTUP) return 3;
+  // 4: the primitive-loop region of a cooperative group (roots, 3*NR I arrays, one 2D table per
+  //    lane that runs a recurrence task, i.e. lanes < min(S, 3*NR*NPARTS)) lies inside the group
+  if (SH::S > 1 && !SH::IS_SLICE) {
+    if (SH::B_ROOTS + SH::B_G + SH::B_SCR > SH::B_GROUP) return 4;
+    if (!SH::REG_RECUR && SH::SM_SCR < cmin(SH::S, 3 * SH::NR * SH::NPARTS) * SH::NIJ * SH::NKL) return 4;
+  }
+  // 5: the two transform buffers lie inside the group region (or the per-block global scratch,
+  //    which then serves exactly one group per block)
+  if (SH::S > 1 && !SH::GLOBAL_BUF && (SH::SM_BUFA + SH::SM_BUFB) * 8 > SH::B_GROUP) return 5;
+  if (SH::GLOBAL_BUF && (SH::Q != 1 || SH::GBUF_PER_BLOCK != SH::SM_BUFA + SH::SM_BUFB)) return 5;
+  // 6: each transform stage's output fits the buffer it is written to: stage j -> B, stage k ->
+  //    A (after stage j) or B, and stage i fills A
+  if (SH::MI * SH::NTUP > SH::SM_BUFA) return 6;
+  if (SH::MI * SH::MJ * SH::NFK * SH::NFL > SH::SM_BUFB) return 6;
+  if (SH::MI * SH::MJ * SH::MK * SH::NFL > (SH::MJ != SH::NFJ ? SH::SM_BUFA : SH::SM_BUFB)) return 6;
+  // 7: group regions keep their alignment and the block's dynamic shared memory is the sum
+  if (SH::B_GROUP % 8 != 0 || (!SH::IS_SLICE && SH::B_GROUP % 16 != 0)) return 7;
+  if (SH::SMEM_BYTES != SH::Q * SH::B_GROUP + SH::TABLE_DOUBLES * 8 || SH::SMEM_BYTES > 227 * 1024) return 7;
+  // 8: named barriers: ids 1..15 and thread counts that are multiples of 32
+  if (!SH::IS_SLICE && SH::S > 32 && (SH::Q > 15 || SH::S % 32 != 0)) return 8;
+  if (SH::IS_SLICE && SH::BLOCK != 32 * SH::LANES && SH::BLOCK / (32 * SH::LANES) > 15) return 8;
+  // 9: a warp-level group's lanes lie in one warp
+  if (!SH::IS_SLICE && SH::S <= 32 && 32 % SH::S != 0) return 9;
+  return 0;
+}
 
 // Group barrier: warp-level for S <= 32, a named barrier per group above.
 template <int S>
@@ -476,6 +520,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   static_assert(!SLICE || (SH::BLOCK % (32 * LN) == 0 && S % PASSES == 0 && !SH::GLOBAL_BUF &&
                            SH::SMEM_BYTES <= 227 * 1024),
                 "sliced shape layout");
+  static_assert(shape_violation<SH>() == 0, "an index of this launch shape can leave its buffer");
   const int group = SLICE ? (int)(threadIdx.x / (32 * LN)) * 32 + (int)(threadIdx.x & 31) : (int)threadIdx.x / S;
   const int lane = SLICE ? (int)(threadIdx.x / 32) % LN : (int)threadIdx.x % S;
   char* sgb = reinterpret_cast<char*>(smem + SH::TABLE_DOUBLES) + group * SH::B_GROUP;

@@ -120,6 +120,35 @@ int load_basis(Basis& b, const int* atm, int natm, const int* bas, int nbas, con
   return CINTX_STATUS_SUCCESS;
 }
 
+// Recurrence centre of a shell pair.  The vertical recurrence is built on one centre X and the
+// horizontal transfer moves angular momentum to the other, Y; the recurrence's coefficient P - X
+// (P the primitive pair's product centre) is a_y/(a_x + a_y) |X - Y| long, and its powers, with
+// the transfer's powers of |X - Y|, cancel down to the integral.  Building on the diffuse shell of
+// a diffuse/tight pair far apart loses most of the digits: a (ff|ff) block of a 0.17 / 2253
+// exponent pair 4 bohr apart is 6% off, while building on the tight shell matches 40-digit
+// arithmetic to 1e-19.  libcint takes the shell of higher l and, for equal l, the second one
+// (ibase = li > lj, g2e.c:101); this library takes the higher l too and, for equal l, the shell
+// with the smaller cancellation measure max over primitive pairs of a_y |X - Y| / sqrt(a_x + a_y)
+// (ties, e.g. one centre: the larger shell index).  Returns true when real shell sx is the
+// recurrence centre of the pair (sx, sy).
+bool pair_base_first(const Basis& B, int sx, int sy) {
+  const ShellInfo& X = B.sh[sx];
+  const ShellInfo& Y = B.sh[sy];
+  if (X.l != Y.l) return X.l > Y.l;
+  if (sx == sy) return true;
+  const double dx = X.r[0] - Y.r[0], dy = X.r[1] - Y.r[1], dz = X.r[2] - Y.r[2];
+  const double d = sqrt(dx * dx + dy * dy + dz * dz);
+  double on_x = 0, on_y = 0;
+  for (double ax : X.exps)
+    for (double ay : Y.exps) {
+      const double r = d / sqrt(ax + ay);
+      on_x = std::max(on_x, ay * r);
+      on_y = std::max(on_y, ax * r);
+    }
+  if (!(on_x != on_y) || fabs(on_x - on_y) <= 1e-12 * std::max(on_x, on_y)) return sx >= sy;
+  return on_x < on_y;
+}
+
 // CINTset_pairdata semantics (optimizer.c:288-342) on virtual shells a (first) and b.
 void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
   const ShellInfo& A = B.sh[B.vshell[a]];
@@ -359,8 +388,9 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
   PairHost ph;
   for (int u = 0; u < npv; ++u) {
     for (int v = 0; v <= u; ++v) {
-      const int lu = B.sh[B.vshell[u]].l, lv = B.sh[B.vshell[v]].l;
-      const int a = lu >= lv ? u : v, b = lu >= lv ? v : u;
+      // recurrence centre first (pair_base_first; contractions of one shell: larger index first)
+      const bool uf = pair_base_first(B, B.vshell[u], B.vshell[v]);
+      const int a = uf ? u : v, b = uf ? v : u;
       build_pair(B, a, b, o->build_cutoff, ph);
       const int id = pair_index(u, v);
       ph.sp.prim_off = (int)prims.size();
@@ -433,18 +463,15 @@ static void make_optimizer(CINTOpt** opt, const int* atm, int natm, const int* b
 }
 
 // ---------------------------------------------------------------- orientation
-// Requested axes 0..3 with angular momenta l[4] (unit axes have l = 0).  Chooses the kernel
-// class and which requested axis feeds each kernel axis.
-static Oriented orient(const int l[4], bool unit_b1, bool unit_b3, int idx0, int idx1, int idx2, int idx3) {
+// Requested axes 0..3 with angular momenta l[4] (unit axes have l = 0) of the real shells
+// idx0..idx3.  Chooses the kernel class and which requested axis feeds each kernel axis.
+static Oriented orient(const Basis& B, const int l[4], bool unit_b1, bool unit_b3, int idx0, int idx1, int idx2,
+                       int idx3) {
   Oriented o;
-  // pair 1 = axes (0,1), pair 2 = axes (2,3); larger l first, equal l: larger shell index first
-  auto pair_first = [&](int la, int lb, int ia, int ib, bool unit_b) {
-    if (unit_b) return true;
-    if (la != lb) return la > lb;
-    return ia >= ib;
-  };
-  const bool f1 = pair_first(l[0], l[1], idx0, idx1, unit_b1);
-  const bool f2 = pair_first(l[2], l[3], idx2, idx3, unit_b3);
+  // pair 1 = axes (0,1), pair 2 = axes (2,3); the recurrence centre of each pair first
+  auto pair_first = [&](int ia, int ib, bool unit_b) { return unit_b || pair_base_first(B, ia, ib); };
+  const bool f1 = pair_first(idx0, idx1, unit_b1);
+  const bool f2 = pair_first(idx2, idx3, unit_b3);
   int p1[2] = {f1 ? 0 : 1, f1 ? 1 : 0};
   int p2[2] = {f2 ? 2 : 3, f2 ? 3 : 2};
   const int l1a = l[p1[0]], l1b = l[p1[1]], l2a = l[p2[0]], l2b = l[p2[1]];
@@ -572,7 +599,7 @@ static int eval_call(int family, bool sph, double* out, int* dims, int* shls, in
   for (int a = 0; a < 4; ++a) block *= counts[a];
 
   // empty check (screening) and host pair construction per contraction tuple
-  const Oriented ori = orient(rl, unit[1], unit[3], rs[0], rs[1], rs[2], rs[3]);
+  const Oriented ori = orient(*B, rl, unit[1], unit[3], rs[0], rs[1], rs[2], rs[3]);
   int rc;
   DeviceState* ds;
   if ((rc = device_state(&ds))) return 0;

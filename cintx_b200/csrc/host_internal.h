@@ -59,6 +59,11 @@ struct PairHost {
   std::vector<int> pa, pb;  // primitive indices (within shells a and b) of each entry of prims
 };
 
+// True when real shell sx is the recurrence centre of the pair (sx, sy): the higher l, and for
+// equal l the shell whose recurrence cancels least (host_api.cpp).  Every pair the kernels see is
+// oriented this way: its first shell is the centre the vertical recurrence is built on.
+bool pair_base_first(const Basis& B, int sx, int sy);
+
 // Builds the screened primitive pairs of virtual shells (a, b), in that order (b < 0: unit).
 void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out);
 

@@ -92,6 +92,19 @@ struct Tile {
   int col0(size_t row) const { return colstart.empty() ? 0 : colstart[row]; }
 };
 
+// Shells of a stored pair in the order a screened plan reports them and lays its blocks out in.
+// The kernels build on the pair's first shell (its recurrence centre, pair_base_first); for equal
+// l the pair is reported the other way round, (other, centre), because libcint builds an equal-l
+// pair on its second shell (g2e.c:101, g3c2e.c:80): evaluated on a reported tuple, libcint then
+// uses the same stable centre.  Unit pairs (3- and 2-centre) report -1 for their missing shell.
+int2 reported_shells(const Opt* o, int id) {
+  const Basis& B = o->basis;
+  const int a = B.vshell[o->pair_a[id]];
+  if (o->pair_b[id] < 0) return make_int2(a, -1);
+  const int b = B.vshell[o->pair_b[id]];
+  return o->pair_la[id] == o->pair_lb[id] ? make_int2(b, a) : make_int2(a, b);
+}
+
 }  // namespace
 
 struct CintxPlan {
@@ -720,8 +733,9 @@ static bool ao_maps(CintxPlan* p, const std::vector<int>& aoloc) {
   if (p->d_psh) return true;
   const Opt* o = p->opt;
   const Basis& B = o->basis;
+  // block axes 0 and 1 of a pair: its shells in reported order (the layout screened plans write)
   std::vector<int2> psh(o->npairs);
-  for (int id = 0; id < o->npairs; ++id) psh[id] = make_int2(B.vshell[o->pair_a[id]], B.vshell[o->pair_b[id]]);
+  for (int id = 0; id < o->npairs; ++id) psh[id] = reported_shells(o, id);
   bool ok = cudaMalloc(&p->d_psh, sizeof(int2) * std::max(o->npairs, 1)) == cudaSuccess &&
             cudaMalloc(&p->d_aoloc, sizeof(int) * aoloc.size()) == cudaSuccess;
   if (ok) {
@@ -878,12 +892,11 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
         if (k >= cap) return CINTX_STATUS_BUFFER_TOO_SMALL;
         const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
         const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
-        const Basis& B = o->basis;
-        // unit pairs (3-centre sweeps) have no second shell: -1
-        quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
-        quartets[k * 4 + 1] = o->pair_b[pa] < 0 ? -1 : B.vshell[o->pair_b[pa]];
-        quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
-        quartets[k * 4 + 3] = o->pair_b[pb] < 0 ? -1 : B.vshell[o->pair_b[pb]];
+        const int2 ra = reported_shells(o, pa), rb = reported_shells(o, pb);
+        quartets[k * 4 + 0] = ra.x;
+        quartets[k * 4 + 1] = ra.y;
+        quartets[k * 4 + 2] = rb.x;
+        quartets[k * 4 + 3] = rb.y;
       }
     }
   }
@@ -931,11 +944,11 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
       const long long q = g - tp[ti];
       const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
       const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
-      // unit pairs (3-centre sweeps) have no second shell: -1
-      quartets[k * 4 + 0] = B.vshell[o->pair_a[pa]];
-      quartets[k * 4 + 1] = o->pair_b[pa] < 0 ? -1 : B.vshell[o->pair_b[pa]];
-      quartets[k * 4 + 2] = B.vshell[o->pair_a[pb]];
-      quartets[k * 4 + 3] = o->pair_b[pb] < 0 ? -1 : B.vshell[o->pair_b[pb]];
+      const int2 ra = reported_shells(o, pa), rb = reported_shells(o, pb);
+      quartets[k * 4 + 0] = ra.x;
+      quartets[k * 4 + 1] = ra.y;
+      quartets[k * 4 + 2] = rb.x;
+      quartets[k * 4 + 3] = rb.y;
     }
   } else {
     const long long total = (long long)p->h_tuples.size() / 4;
@@ -1708,6 +1721,9 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
       t.lk = std::get<0>(tkeys[Bt]);
       t.ll = std::get<1>(tkeys[Bt]);
       t.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
+      // equal-l pairs are reported (other, centre): their two axes trade strides
+      if (t.li == t.lj) std::swap(t.st.s0, t.st.s1);
+      if (t.lk == t.ll) std::swap(t.st.s2, t.st.s3);
       const std::vector<int>& rows = tlist[A];
       const std::vector<int>& cols = tlist[Bt];
       std::vector<double> qcols(cols.size());
@@ -1882,9 +1898,11 @@ int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, 
       if (!t.swap) {
         t.li = la; t.lj = lb; t.lk = lk; t.ll = 0;
         t.st.s0 = 1; t.st.s1 = ni; t.st.s2 = ni * nj; t.st.s3 = 0;
+        if (la == lb) std::swap(t.st.s0, t.st.s1);  // equal-l pairs are reported (other, centre)
       } else {
         t.li = lk; t.lj = 0; t.lk = la; t.ll = lb;
         t.st.s0 = ni * nj; t.st.s1 = 0; t.st.s2 = 1; t.st.s3 = ni;
+        if (la == lb) std::swap(t.st.s2, t.st.s3);
       }
       t.row_prefix.push_back(0);
       for (int r : rows) {

@@ -118,15 +118,15 @@ extern "C" int cintx_int2e_noalloc(double* out_dev, const int* shls, int64_t n, 
   const double cutoff = expcutoff_2e(B.env.data());
   auto next = [&](int l) { return sp ? 2 * l + 1 : (l + 1) * (l + 2) / 2; };
 
-  // screened pairs, oriented larger l first (equal l: larger virtual index first)
+  // screened pairs, oriented with their recurrence centre first (pair_base_first; contractions
+  // of one shell: larger virtual index first), as the optimizer orients them
   std::map<std::pair<int, int>, int> pair_id;
   std::vector<ShellPair> pairs;
   std::vector<PrimPair> prims;
   std::vector<int> pair_l1, pair_l2;
   PairHost ph;
   auto get_pair = [&](int x, int y, bool& x_first) {
-    const int lx = B.sh[B.vshell[x]].l, ly = B.sh[B.vshell[y]].l;
-    x_first = lx != ly ? lx > ly : x >= y;
+    x_first = B.vshell[x] != B.vshell[y] ? pair_base_first(B, B.vshell[x], B.vshell[y]) : x >= y;
     const int a = x_first ? x : y, b = x_first ? y : x;
     auto key = std::make_pair(a, b);
     auto it = pair_id.find(key);

@@ -12,7 +12,9 @@
  *     common_factor = pi^3 * 2/sqrt(pi) * prod common_fac_sp(l)    (g2e.c:54-56, g1e.c:566);
  *   - the Rys coefficients b00, b10, b01, c00, c0p of g2e.c:4542-4565 written in t^2 form;
  *   - the 2D vertical recurrence (CINTg0_2e_2d, g2e.c:272) built on centres i and k and the
- *     horizontal transfer to j and l (the HRR of g2e.c:428-694 with a fixed base choice);
+ *     horizontal transfer to j and l (the HRR of g2e.c:428-694), with each pair's shells taken in
+ *     the order that puts the recurrence on its stable centre (base_first) and the block
+ *     transposed back to the requested order;
  *   - the cartesian product sum of CINTgout2e (cint2e.c:961) and contraction (g1e.c:509);
  *   - the cartesian -> spherical transform of c2s_sph_2e1 (cart2sph.c:5324) / c2s_sph_3c2e1
  *     (cart2sph.c:5884) / c2s_sph_1e (cart2sph.c:4833).
@@ -480,12 +482,94 @@ static int run(int sph, double *out, int nsh, const int *shls, const int *atm, c
         return ok;
 }
 
+/*
+ * Recurrence centre of the pair (sx, sy): the shell of higher l and, for equal l, the one whose
+ * recurrence cancels least, i.e. the smaller max over primitive pairs of a_y |X - Y| /
+ * sqrt(a_x + a_y) (ties: the larger shell index).  libcint builds on the higher l and, for equal
+ * l, on the second shell (ibase = li > lj, g2e.c:101); on a diffuse/tight pair far apart that
+ * choice loses digits to cancellation (a (ff|ff) block of a 0.17 / 2253 exponent pair 4 bohr apart
+ * is 6% off), so this restatement takes the stable centre and transposes the block back.
+ */
+static int base_first(int sx, int sy, const int *atm, const int *bas, const double *env)
+{
+        Shell x, y;
+        load_shell(&x, sx, atm, bas, env);
+        load_shell(&y, sy, atm, bas, env);
+        if (x.l != y.l) {
+                return x.l > y.l;
+        }
+        if (sx == sy) {
+                return 1;
+        }
+        double d = sqrt((x.r[0] - y.r[0]) * (x.r[0] - y.r[0]) + (x.r[1] - y.r[1]) * (x.r[1] - y.r[1]) +
+                        (x.r[2] - y.r[2]) * (x.r[2] - y.r[2]));
+        double on_x = 0, on_y = 0;
+        for (int p = 0; p < x.nprim; p++) {
+                for (int q = 0; q < y.nprim; q++) {
+                        double r = d / sqrt(x.ai[p] + y.ai[q]);
+                        on_x = fmax(on_x, y.ai[q] * r);
+                        on_y = fmax(on_y, x.ai[p] * r);
+                }
+        }
+        if (!(on_x != on_y) || fabs(on_x - on_y) <= 1e-12 * fmax(on_x, on_y)) {
+                return sx >= sy;
+        }
+        return on_x < on_y;
+}
+
+static int axis_len(int sh, const int *bas, int sph)
+{
+        int l = bas[BAS_SLOTS * sh + 1];
+        return (sph ? 2 * l + 1 : ncart(l)) * bas[BAS_SLOTS * sh + 3];
+}
+
+/* run() on the shells in stable-centre order, with the block written in the requested order */
+static int run_oriented(int sph, double *out, int nsh, const int *shls, const int *atm, const int *bas,
+                        const double *env)
+{
+        int ord[4] = {0, 1, 2, 3};
+        if (nsh >= 3 && !base_first(shls[0], shls[1], atm, bas, env)) {
+                ord[0] = 1;
+                ord[1] = 0;
+        }
+        if (nsh == 4 && !base_first(shls[2], shls[3], atm, bas, env)) {
+                ord[2] = 3;
+                ord[3] = 2;
+        }
+        if (ord[0] == 0 && ord[2] == 2) {
+                return run(sph, out, nsh, shls, atm, bas, env);
+        }
+        int s2[4], n[4] = {1, 1, 1, 1};
+        for (int a = 0; a < nsh; a++) {
+                s2[a] = shls[ord[a]];
+                n[a] = axis_len(shls[a], bas, sph);
+        }
+        size_t tot = (size_t)n[0] * n[1] * n[2] * n[3];
+        double *tmp = malloc(sizeof(double) * tot);
+        int ok = run(sph, tmp, nsh, s2, atm, bas, env);
+        /* tmp axis a is requested axis ord[a] */
+        int m[4];
+        for (int a = 0; a < 4; a++) {
+                m[a] = n[ord[a]];
+        }
+        for (size_t e = 0; e < tot; e++) {
+                size_t r = e, idx[4];
+                for (int a = 0; a < 4; a++) {
+                        idx[ord[a]] = r % m[a];
+                        r /= m[a];
+                }
+                out[idx[0] + n[0] * (idx[1] + n[1] * (idx[2] + n[2] * idx[3]))] = tmp[e];
+        }
+        free(tmp);
+        return ok;
+}
+
 int oracle_int2e(int sph, double *out, const int *shls, const int *atm, int natm,
                  const int *bas, int nbas, const double *env)
 {
         (void)natm;
         (void)nbas;
-        return run(sph, out, 4, shls, atm, bas, env);
+        return run_oriented(sph, out, 4, shls, atm, bas, env);
 }
 
 int oracle_int3c2e(int sph, double *out, const int *shls, const int *atm, int natm,
@@ -493,7 +577,7 @@ int oracle_int3c2e(int sph, double *out, const int *shls, const int *atm, int na
 {
         (void)natm;
         (void)nbas;
-        return run(sph, out, 3, shls, atm, bas, env);
+        return run_oriented(sph, out, 3, shls, atm, bas, env);
 }
 
 int oracle_int2c2e(int sph, double *out, const int *shls, const int *atm, int natm,

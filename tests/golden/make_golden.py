@@ -9,7 +9,9 @@
                      generally-contracted basis (nctr = 2) and dims / expcutoff variants.
   libcint_mol120f.npz  libcint blocks of 50 quartets from every f-containing angular-momentum
                      class of the 120-atom molecule's Schwarz-screened quartet set, each quartet
-                     in a random one of its 8 index orders.
+                     in a random one of its 8 index orders (libcint evaluated with each equal-l
+                     pair ordered so that it builds on the pair's stable centre, then transposed
+                     to the stored order: libcint_stable).
 
 Run from the repository root: python tests/golden/make_golden.py   (needs oracle/_ref)
 """
@@ -212,16 +214,72 @@ def class_stratified_quartets(ref, mol, cutoff, per_class, seed, need_l=3):
     return out
 
 
+def base_first(mol, sx, sy):
+    """The shell of the pair (sx, sy) a numerically stable recurrence is built on: the higher l,
+    and for equal l the smaller cancellation measure max over primitive pairs of
+    a_y |X - Y| / sqrt(a_x + a_y) (ties: the larger shell index).  libcint builds on the second
+    shell of an equal-l pair (g2e.c:101), so it evaluates a tuple stably when the pair's stable
+    centre comes second."""
+    lx, ly = int(mol.bas[sx, 1]), int(mol.bas[sy, 1])
+    if lx != ly:
+        return lx > ly
+    if sx == sy:
+        return True
+    def shell(s):
+        b = mol.bas[s]
+        return mol.env[b[5]:b[5] + b[2]], mol.env[mol.atm[b[0], 1]:mol.atm[b[0], 1] + 3]
+    (ax, rx), (ay, ry) = shell(sx), shell(sy)
+    d = float(np.linalg.norm(rx - ry))
+    r = d / np.sqrt(ax[:, None] + ay[None, :])
+    on_x = float((ay[None, :] * r).max())
+    on_y = float((ax[:, None] * r).max())
+    if not (on_x != on_y) or abs(on_x - on_y) <= 1e-12 * max(on_x, on_y):
+        return sx >= sy
+    return on_x < on_y
+
+
+def libcint_stable(ref, mol, tuples, sph=True):
+    """libcint blocks of int2e tuples in the requested index order, each evaluated with every
+    equal-l pair ordered (other, stable centre) so that libcint builds its recurrence on the
+    stable centre (unequal-l pairs are left as requested: libcint builds on the higher l either
+    way), then transposed back.  Returns (values, offsets[n+1], return values)."""
+    tuples = np.ascontiguousarray(tuples, dtype=np.int32)
+    ords = []
+    for t in tuples:
+        o = [0, 1, 2, 3]
+        for a, b in ((0, 1), (2, 3)):
+            la, lb = mol.bas[t[a], 1], mol.bas[t[b], 1]
+            # libcint builds on the second shell of an equal-l pair: put the stable centre there
+            if la == lb and base_first(mol, t[a], t[b]):
+                o[a], o[b] = b, a
+        ords.append(o)
+    ords = np.array(ords)
+    ev = tuples[np.arange(len(tuples))[:, None], ords]
+    vals, offs, rets = ref.batch(ev, mol, sph)
+    out = np.empty_like(vals)
+    l = mol.bas[:, 1]
+    nc = mol.bas[:, 3]
+    per = (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
+    for q, (t, o) in enumerate(zip(tuples, ords)):
+        n = per[t]                                  # requested axis lengths
+        blk = vals[offs[q]:offs[q + 1]].reshape([n[o[3]], n[o[2]], n[o[1]], n[o[0]]])
+        # blk axes (slowest first) are requested axes o[3], o[2], o[1], o[0]; order them as 3, 2, 1, 0
+        pos = {o[3 - k]: k for k in range(4)}
+        out[offs[q]:offs[q + 1]] = blk.transpose([pos[3], pos[2], pos[1], pos[0]]).reshape(-1)
+    return out, offs, rets
+
+
 def make_mol120():
     """libcint blocks for a class-stratified sample of the 120-atom f-shell molecule's Schwarz-
-    screened (1e-12) quartet set: 50 quartets of every class containing an f shell."""
+    screened (1e-12) quartet set: 50 quartets of every class containing an f shell, evaluated by
+    libcint in the index order that makes it build on each pair's stable centre."""
     ref = RefLibcint()
     mol = M.mol120()
     per = class_stratified_quartets(ref, mol, 1e-12, 50, 120)
     labels = sorted(per)
     tuples = np.concatenate([per[k] for k in labels])
     cls = np.concatenate([np.full(len(per[k]), i, dtype=np.int32) for i, k in enumerate(labels)])
-    vals, offs, rets = ref.batch(tuples, mol)
+    vals, offs, rets = libcint_stable(ref, mol, tuples)
     np.savez_compressed(os.path.join(HERE, "libcint_mol120f.npz"), int2e_sph_tuples=tuples,
                         int2e_sph_offsets=offs, int2e_sph_values=vals, int2e_sph_ret=rets,
                         class_index=cls, class_labels=np.array(labels))
