@@ -20,7 +20,7 @@ INT2E, INT3C2E, INT2C2E = 0, 1, 2
 
 _API = {"CintxError", "Optimizer", "Plan", "int2c2e_cart", "int2c2e_sph", "int2e_cart", "int2e_sph",
         "int3c2e_cart", "int3c2e_sph", "lib", "launch_count", "rys_roots", "rys_t2_batch", "last_error",
-        "RysNet"}
+        "RysNet", "ao_loc"}
 
 
 def __getattr__(name):

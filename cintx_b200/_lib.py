@@ -85,6 +85,17 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_execute_host_ring.restype = _i
     L.cintx_plan_execute_s8.argtypes = [_vp, _vp, _i64, _vp]
     L.cintx_plan_execute_s8.restype = _i
+    L.cintx_plan_execute_ao.argtypes = [_vp, _i, _vp, _i64, _vp]
+    L.cintx_plan_execute_ao.restype = _i
+    for name in ("CINTcgto_cart", "CINTcgto_spheric"):
+        getattr(L, name).argtypes = [_i, _ip]
+        getattr(L, name).restype = _i
+    for name in ("CINTtot_cgto_spheric", "CINTtot_cgto_cart"):
+        getattr(L, name).argtypes = [_ip, _i]
+        getattr(L, name).restype = _i
+    for name in ("CINTshells_spheric_offset", "CINTshells_cart_offset"):
+        getattr(L, name).argtypes = [_ip, _ip, _i]
+        getattr(L, name).restype = None
     L.cintx_plan_jk.argtypes = [_vp, _vp, _i, _vp, _vp, _vp]
     L.cintx_plan_jk.restype = _i
     L.cintx_plan_autotune.argtypes = [_vp, _i64, ctypes.c_void_p, ctypes.c_void_p, _i]
@@ -200,6 +211,18 @@ def int2c2e_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
 
 def int2c2e_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
     return _call("int2c2e_cart", 2, shls, atm, bas, env, opt, dims, out, False)
+
+
+def ao_loc(bas, sph: bool = True) -> np.ndarray:
+    """AO offsets of the shells (nbas + 1 entries, the last one the total), from the library's
+    CINTshells_spheric_offset / CINTshells_cart_offset and CINTtot_cgto_*."""
+    b = np.ascontiguousarray(bas, dtype=np.int32)
+    n = b.shape[0]
+    loc = np.zeros(n + 1, dtype=np.int32)
+    (lib.CINTshells_spheric_offset if sph else lib.CINTshells_cart_offset)(loc.ctypes.data_as(_ip),
+                                                                           b.ctypes.data_as(_ip), n)
+    loc[n] = (lib.CINTtot_cgto_spheric if sph else lib.CINTtot_cgto_cart)(b.ctypes.data_as(_ip), n)
+    return loc
 
 
 def rys_roots(n: int, x: float):
@@ -375,6 +398,12 @@ class Plan:
     def execute_s8(self, eri_ptr: int, length: int, stream: int = 0):
         """The sweep as the 8-fold packed AO tensor at device pointer eri_ptr (length doubles)."""
         _check(lib.cintx_plan_execute_s8(self.handle, ctypes.c_void_p(eri_ptr), int(length), ctypes.c_void_p(stream)))
+
+    def execute_ao(self, eri_ptr: int, length: int, aosym: int = 1, stream: int = 0):
+        """The sweep as an AO-indexed tensor at device pointer eri_ptr (length doubles): aosym 1 the
+        full nao^4 tensor, 4 the npair x npair pair matrix, 8 the 8-fold packed triangle."""
+        _check(lib.cintx_plan_execute_ao(self.handle, int(aosym), ctypes.c_void_p(eri_ptr), int(length),
+                                         ctypes.c_void_p(stream)))
 
     def use_tuned_shapes(self) -> int:
         """Reuse the launch shapes autotuned earlier in this process; returns segments changed."""

@@ -708,6 +708,36 @@ using namespace cintx;
 
 extern "C" {
 
+// Basis bookkeeping of libcint (cint_bas.c:36-155): functions per shell and AO offsets.  As in
+// libcint, the offset routines write ao_loc[0..nbas-1] only (the total comes from CINTtot_*).
+int CINTcgto_cart(const int bas_id, const int* bas) {
+  const int l = bas[bas_id * BAS_SLOTS + ANG_OF];
+  return (l + 1) * (l + 2) / 2 * bas[bas_id * BAS_SLOTS + NCTR_OF];
+}
+int CINTcgto_spheric(const int bas_id, const int* bas) {
+  return (2 * bas[bas_id * BAS_SLOTS + ANG_OF] + 1) * bas[bas_id * BAS_SLOTS + NCTR_OF];
+}
+int CINTtot_cgto_spheric(const int* bas, const int nbas) {
+  int n = 0;
+  for (int i = 0; i < nbas; ++i) n += CINTcgto_spheric(i, bas);
+  return n;
+}
+int CINTtot_cgto_cart(const int* bas, const int nbas) {
+  int n = 0;
+  for (int i = 0; i < nbas; ++i) n += CINTcgto_cart(i, bas);
+  return n;
+}
+void CINTshells_spheric_offset(int ao_loc[], const int* bas, const int nbas) {
+  if (nbas <= 0) return;
+  ao_loc[0] = 0;
+  for (int i = 1; i < nbas; ++i) ao_loc[i] = ao_loc[i - 1] + CINTcgto_spheric(i - 1, bas);
+}
+void CINTshells_cart_offset(int ao_loc[], const int* bas, const int nbas) {
+  if (nbas <= 0) return;
+  ao_loc[0] = 0;
+  for (int i = 1; i < nbas; ++i) ao_loc[i] = ao_loc[i - 1] + CINTcgto_cart(i - 1, bas);
+}
+
 int int2e_sph(double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas, double* env,
               CINTOpt* opt, double* cache) {
   (void)cache;

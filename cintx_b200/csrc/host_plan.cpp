@@ -39,6 +39,8 @@ cudaError_t launch_jk_contract(const QuartetRec* recs, long long nrec, const int
 cudaError_t launch_symmetrize(const double* X, double* M, int n, cudaStream_t stream);
 cudaError_t launch_scatter_s8(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
                               const double* out, double* eri, cudaStream_t stream);
+cudaError_t launch_scatter_ao(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                              const double* out, double* eri, int mode, long long nao, cudaStream_t stream);
 }
 
 using namespace cintx;
@@ -746,22 +748,31 @@ static bool ao_maps(CintxPlan* p, const std::vector<int>& aoloc) {
 }
 
 int cintx_plan_execute_s8(CintxPlan* p, double* eri, int64_t len, void* stream_) {
+  return cintx_plan_execute_ao(p, 8, eri, len, stream_);
+}
+
+int cintx_plan_execute_ao(CintxPlan* p, int aosym, double* eri, int64_t len, void* stream_) {
   clear_error();
   if (!p || !eri) {
     set_error(CINTX_STATUS_NULL_POINTER, "plan and eri must not be NULL");
     return CINTX_STATUS_NULL_POINTER;
   }
   if (p->tiles.empty() || p->family != CINTX_INT2E) {
-    set_error(CINTX_STATUS_UNSUPPORTED_API, "the packed AO tensor is written from an int2e unique-quartet sweep");
+    set_error(CINTX_STATUS_UNSUPPORTED_API, "the AO tensor is written from an int2e unique-quartet sweep");
     return CINTX_STATUS_UNSUPPORTED_API;
+  }
+  if (aosym != 1 && aosym != 4 && aosym != 8) {
+    set_error(CINTX_STATUS_INVALID_INPUT, "aosym must be 1, 4 or 8");
+    return CINTX_STATUS_INVALID_INPUT;
   }
   const Basis& B = p->opt->basis;
   std::vector<int> aoloc(B.nbas + 1, 0);
   for (int sh = 0; sh < B.nbas; ++sh) aoloc[sh + 1] = aoloc[sh] + nsph_or_cart(B.sh[sh].l, p->sph);
-  const long long nao = aoloc[B.nbas], npair = nao * (nao + 1) / 2, need = npair * (npair + 1) / 2;
+  const long long nao = aoloc[B.nbas], npair = nao * (nao + 1) / 2;
+  const long long need = aosym == 8 ? npair * (npair + 1) / 2 : (aosym == 4 ? npair * npair : nao * nao * nao * nao);
   if (len < need) {
-    set_error(CINTX_STATUS_BUFFER_TOO_SMALL, "the packed tensor of " + std::to_string(nao) + " functions needs " +
-                                                 std::to_string(need) + " doubles");
+    set_error(CINTX_STATUS_BUFFER_TOO_SMALL, "the s" + std::to_string(aosym) + " tensor of " + std::to_string(nao) +
+                                                 " functions needs " + std::to_string(need) + " doubles");
     return CINTX_STATUS_BUFFER_TOO_SMALL;
   }
   cudaStream_t stream = (cudaStream_t)stream_;
@@ -775,14 +786,18 @@ int cintx_plan_execute_s8(CintxPlan* p, double* eri, int64_t len, void* stream_)
     if (!ok) p->d_stage = nullptr;
   }
   if (!ok) {
-    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the packed tensor failed");
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "device allocation for the AO tensor failed");
     return CINTX_STATUS_ALLOCATION_FAILED;
   }
   cudaMemsetAsync(eri, 0, sizeof(double) * need, stream);  // quartets below the cutoff stay 0
   for (int64_t c = 0; c < (int64_t)p->chunks.size(); ++c) {
     int rc = cintx_plan_execute(p, c, p->d_stage, stream);
     if (rc) return rc;
-    if (launch_scatter_s8(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc, p->d_stage, eri, stream) != cudaSuccess) {
+    const cudaError_t e = aosym == 8 ? launch_scatter_s8(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc,
+                                                         p->d_stage, eri, stream)
+                                     : launch_scatter_ao(p->d_recs, p->chunks[c].nrec, p->d_psh, p->d_aoloc,
+                                                         p->d_stage, eri, aosym, nao, stream);
+    if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, "scatter launch failed");
       return CINTX_STATUS_EXECUTION_FAILED;
     }

@@ -210,6 +210,49 @@ __global__ void scatter_s8_kernel(const QuartetRec* __restrict__ recs, long long
   }
 }
 
+// Scatters one chunk of a unique-quartet sweep into an unpacked AO tensor, one warp per quartet
+// block: mode 1 (PySCF ao2mo "s1") eri[((p*nao + q)*nao + r)*nao + s] at all eight index orders
+// the quartet stands for; mode 4 ("s4") the pair-pair matrix eri[pq*npair + rs] and its transpose
+// slot, pq = p*(p+1)/2 + q over p >= q.  Slots reached twice receive equal elements.
+__global__ void scatter_ao_kernel(const QuartetRec* __restrict__ recs, long long nrec, const int2* __restrict__ psh,
+                                  const int* __restrict__ aoloc, const double* __restrict__ out,
+                                  double* __restrict__ eri, int mode, long long nao) {
+  const int lane = threadIdx.x & 31;
+  const long long npair = nao * (nao + 1) / 2;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nrec;
+       r += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const QuartetRec rec = recs[r];
+    const int2 ab = psh[rec.pij], cd = psh[rec.pkl];
+    const int i0 = aoloc[ab.x], j0 = aoloc[ab.y], k0 = aoloc[cd.x], l0 = aoloc[cd.y];
+    const int ni = aoloc[ab.x + 1] - i0, nj = aoloc[ab.y + 1] - j0;
+    const int nk = aoloc[cd.x + 1] - k0, nl = aoloc[cd.y + 1] - l0;
+    const int n = ni * nj * nk * nl;
+    const double* v = out + rec.out;
+    for (int e = lane; e < n; e += 32) {
+      const int i = e % ni, j = (e / ni) % nj, k = (e / (ni * nj)) % nk, l = e / (ni * nj * nk);
+      const long long p = i0 + i, q = j0 + j, u = k0 + k, w = l0 + l;
+      const double x = v[e];
+      if (mode == 1) {
+        const long long pq = p * nao + q, qp = q * nao + p, uw = u * nao + w, wu = w * nao + u;
+        const long long n2 = nao * nao;
+        eri[pq * n2 + uw] = x;
+        eri[qp * n2 + uw] = x;
+        eri[pq * n2 + wu] = x;
+        eri[qp * n2 + wu] = x;
+        eri[uw * n2 + pq] = x;
+        eri[wu * n2 + pq] = x;
+        eri[uw * n2 + qp] = x;
+        eri[wu * n2 + qp] = x;
+      } else {
+        const long long pq = p >= q ? p * (p + 1) / 2 + q : q * (q + 1) / 2 + p;
+        const long long uw = u >= w ? u * (u + 1) / 2 + w : w * (w + 1) / 2 + u;
+        eri[pq * npair + uw] = x;
+        eri[uw * npair + pq] = x;
+      }
+    }
+  }
+}
+
 // As jk_contract_kernel for small blocks (all of one class, n = ni nj nk nl <= 32 elements): one
 // thread per quartet, so the many tiny blocks ((ss|ss), (ps|ss), ...) do not idle a warp each.
 __global__ void jk_contract_small_kernel(const QuartetRec* __restrict__ recs, long long nrec,
@@ -323,6 +366,15 @@ cudaError_t launch_scatter_s8(const QuartetRec* recs, long long nrec, const int2
   long long blocks = (nrec * 32 + 255) / 256;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   scatter_s8_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, eri);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_ao(const QuartetRec* recs, long long nrec, const int2* psh, const int* aoloc,
+                              const double* out, double* eri, int mode, long long nao, cudaStream_t stream) {
+  if (nrec <= 0) return cudaSuccess;
+  long long blocks = (nrec * 32 + 255) / 256;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  scatter_ao_kernel<<<(unsigned)blocks, 256, 0, stream>>>(recs, nrec, psh, aoloc, out, eri, mode, nao);
   return cudaGetLastError();
 }
 

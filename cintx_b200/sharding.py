@@ -27,6 +27,27 @@ def chunks_of(owner, rank: int):
     return [c for c, r in enumerate(owner) if r == rank]
 
 
+def plan_digest(plan, world: int) -> dict:
+    """What a rank needs to agree on with the others before it takes its share of a sweep: the
+    plan's chunk sizes, each chunk's kernel-class segments and a hash of its quartet list, and the
+    chunk assignment for `world` ranks with each rank's integral count."""
+    import hashlib
+
+    import numpy as np
+    st = plan.stats
+    h = hashlib.sha256()
+    sizes, segs = [], []
+    for c in range(st.nchunks):
+        sizes.append(plan.chunk_size(c))
+        cls, nq, fl = plan.segments(c)
+        segs.append([tuple(int(v) for v in cl) + (int(n),) for cl, n in zip(cls, nq)])
+        h.update(np.ascontiguousarray(plan.chunk_quartets(c)).tobytes())
+    owner = assign_chunks([float(plan.segments(c)[2].sum()) for c in range(st.nchunks)], world)
+    shard_ints = [sum(sizes[c] for c in chunks_of(owner, r)) for r in range(world)]
+    return {"nquartets": int(st.nquartets), "nintegrals": int(st.nintegrals), "chunk_sizes": sizes,
+            "segments": segs, "quartets_sha256": h.hexdigest(), "owner": owner, "shard_integrals": shard_ints}
+
+
 def max_over_ranks(value: float, device=None) -> float:
     """Max of a per-rank scalar over the default process group (the value itself when the
     group is not initialised)."""

@@ -73,6 +73,20 @@ CINTX_API void CINTdel_optimizer(CINTOpt **opt);
  * order nroots (1..9), evaluated by the device root evaluator.  Returns 0 on success. */
 CINTX_API int CINTrys_roots(int nroots, double x, double *u, double *w);
 
+/* Basis bookkeeping, as libcint's cint_bas.c (the AO offsets a caller lays AO-indexed tensors out
+ * with; cintx-compat helpers.rs:150-200 restates them):
+ *   CINTcgto_cart / CINTcgto_spheric (cint_bas.c:36, :49): functions of shell bas_id,
+ *     ncart(l) * nctr or (2l+1) * nctr;
+ *   CINTtot_cgto_spheric / CINTtot_cgto_cart (cint_bas.c:108, :124): functions of all nbas shells;
+ *   CINTshells_spheric_offset / CINTshells_cart_offset (cint_bas.c:149, :141): ao_loc[i] = first
+ *     function of shell i, for i < nbas (ao_loc[nbas] is not written, as in libcint). */
+CINTX_API int CINTcgto_cart(const int bas_id, const int *bas);
+CINTX_API int CINTcgto_spheric(const int bas_id, const int *bas);
+CINTX_API int CINTtot_cgto_spheric(const int *bas, const int nbas);
+CINTX_API int CINTtot_cgto_cart(const int *bas, const int nbas);
+CINTX_API void CINTshells_spheric_offset(int ao_loc[], const int *bas, const int nbas);
+CINTX_API void CINTshells_cart_offset(int ao_loc[], const int *bas, const int nbas);
+
 /* Device root evaluator over many points (no libcint counterpart; used to verify the root
  * table): t2w[i*2n + r] = t_r^2 and t2w[i*2n + n + r] = w_r at x[i].  Host arrays. */
 CINTX_API int cintx_rys_t2_batch(int nroots, const double *x, int64_t nx, double *t2w);
@@ -206,6 +220,14 @@ CINTX_API int cintx_plan_jk(CintxPlan *plan, const double *dm, int nao, double *
  * pq >= rs; len >= npair*(npair+1)/2 doubles of device memory, npair = nao*(nao+1)/2.  Quartets
  * below the plan's cutoff are 0.  Asynchronous on stream. */
 CINTX_API int cintx_plan_execute_s8(CintxPlan *plan, double *eri, int64_t len, void *stream);
+
+/* The whole sweep as an AO-indexed tensor in one of PySCF ao2mo's layouts (AOs ordered by shell in
+ * this plan's representation, offsets as CINTshells_*_offset), quartets below the plan's cutoff 0:
+ *   aosym 1 ("s1"): eri[((p*nao + q)*nao + r)*nao + s], nao^4 doubles;
+ *   aosym 4 ("s4"): eri[pq*npair + rs], pq = p*(p+1)/2 + q (p >= q), rs likewise, npair^2 doubles;
+ *   aosym 8 ("s8"): as cintx_plan_execute_s8.
+ * len (doubles of device memory at eri) must hold the layout.  Asynchronous on stream. */
+CINTX_API int cintx_plan_execute_ao(CintxPlan *plan, int aosym, double *eri, int64_t len, void *stream);
 
 /* Plan statistics. */
 typedef struct {

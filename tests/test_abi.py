@@ -124,3 +124,36 @@ def test_cintrs_dispatch_statuses_without_device_work():
               ctypes.byref(summ)) == 1  # env shorter than the basis needs
     code, msg = _lib.last_error()
     assert code == 1 and "env" in msg
+
+
+def test_basis_offsets_match_libcint():
+    """CINTshells_*_offset / CINTtot_cgto_* / CINTcgto_* (host-only, no device work) against libcint
+    built from the reference sources, on a basis with general contractions."""
+    import numpy as np
+    import pytest
+    from cintx_b200 import _lib
+    from cintx_b200 import molecules as M
+    from oracle import RefLibcint
+    g = np.load(os.path.join(ROOT, "tests", "golden", "libcint_ctr2.npz"))
+    for bas in (M.mol120().bas, np.ascontiguousarray(g["bas"], dtype=np.int32)):
+        n = bas.shape[0]
+        for sph in (True, False):
+            loc = _lib.ao_loc(bas, sph)
+            want = np.concatenate([[0], np.cumsum([(2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * c
+                                                   for l, c in zip(bas[:, 1], bas[:, 3])])])
+            assert np.array_equal(loc, want)
+            if RefLibcint.available():
+                ref = ctypes.CDLL(RefLibcint.path)
+                rl = np.full(n + 1, -7, dtype=np.int32)
+                f = ref.CINTshells_spheric_offset if sph else ref.CINTshells_cart_offset
+                f(rl.ctypes.data_as(_lib._ip), bas.ctypes.data_as(_lib._ip), ctypes.c_int(n))
+                assert np.array_equal(rl[:n], loc[:n]) and rl[n] == -7  # ao_loc[nbas] untouched
+                tot = (ref.CINTtot_cgto_spheric if sph else ref.CINTtot_cgto_cart)(bas.ctypes.data_as(_lib._ip),
+                                                                                   ctypes.c_int(n))
+                assert tot == loc[n]
+                cg = ref.CINTcgto_spheric if sph else ref.CINTcgto_cart
+                mine = _lib.lib.CINTcgto_spheric if sph else _lib.lib.CINTcgto_cart
+                for s in range(0, n, 7):
+                    assert cg(ctypes.c_int(s), bas.ctypes.data_as(_lib._ip)) == mine(s, bas.ctypes.data_as(_lib._ip))
+    if not RefLibcint.available():
+        pytest.skip("libcint from the reference sources not built")

@@ -118,3 +118,40 @@ def test_s8_packed_tensor_matches_dense_eri(cx, name):
     ii, jj = np.tril_indices(npair)
     want = ref[ii, jj]
     assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max(), np.abs(got - want).max()
+
+
+@pytest.mark.parametrize("name", ["water3", "jk4"])
+def test_s1_and_s4_tensors_match_dense_eri(cx, name):
+    """cintx_plan_execute_ao with aosym 1 (every index order of every quartet, nao^4) and aosym 4
+    (the pair-pair matrix), slot by slot against the dense oracle tensor (1e-9 of its largest
+    element, as for s8) and against each other; a short buffer is rejected."""
+    import torch
+    from oracle import Restatement
+    orc = Restatement()
+    mol = M.water_like() if name == "water3" else M.random_molecule("jk4", 9, 4, 5.0, with_f=True)
+    eri, n = _dense_eri(orc, mol, True)
+    npair = n * (n + 1) // 2
+    assert np.array_equal(cx.ao_loc(mol.bas, True), mol.ao_loc())
+    tol = 1e-9 * np.abs(eri).max()
+    with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+        plan = cx.Plan.screened(opt, 1e-14, sph=True, max_chunk_doubles=1 << 12)
+        s = torch.cuda.current_stream()
+        b1 = torch.full((n ** 4,), float("nan"), dtype=torch.float64, device="cuda")
+        plan.execute_ao(b1.data_ptr(), b1.numel(), aosym=1, stream=s.cuda_stream)
+        b4 = torch.full((npair * npair,), float("nan"), dtype=torch.float64, device="cuda")
+        plan.execute_ao(b4.data_ptr(), b4.numel(), aosym=4, stream=s.cuda_stream)
+        s.synchronize()
+        with pytest.raises(cx.CintxError):
+            plan.execute_ao(b4.data_ptr(), b4.numel() - 1, aosym=4, stream=s.cuda_stream)
+        with pytest.raises(cx.CintxError):
+            plan.execute_ao(b4.data_ptr(), b4.numel(), aosym=2, stream=s.cuda_stream)
+        plan.close()
+    g1 = b1.cpu().numpy().reshape(n, n, n, n)
+    g4 = b4.cpu().numpy().reshape(npair, npair)
+    assert np.isfinite(g1).all() and np.isfinite(g4).all()
+    assert np.abs(g1 - eri).max() <= tol, np.abs(g1 - eri).max()
+    p, q = np.tril_indices(n)
+    assert np.abs(g4 - eri[p[:, None], q[:, None], p[None, :], q[None, :]]).max() <= tol
+    # the same block elements fill both (a diagonal shell pair reaches a slot from two elements
+    # computed separately, equal to the last bits)
+    assert np.abs(g4 - g1[p[:, None], q[:, None], p[None, :], q[None, :]]).max() <= 1e-13 * np.abs(eri).max()
