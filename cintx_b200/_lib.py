@@ -40,7 +40,14 @@ def _load() -> ctypes.CDLL:
         f = getattr(L, name)
         f.argtypes = sig
         f.restype = _i
-    for name in ("int2e_optimizer", "int3c2e_optimizer", "int2c2e_optimizer"):
+    for name in ("int2e_ip1_sph", "int2e_ip1_cart", "int3c2e_ip1_sph", "int3c2e_ip1_cart"):
+        f = getattr(L, name)
+        f.argtypes = sig
+        f.restype = _i
+    L.cintx_ip1_eval.argtypes = [_i, _vp, _ip, _i64, _i, _ip, _i, _ip, _i, _dp, _i64p]
+    L.cintx_ip1_eval.restype = _i
+    for name in ("int2e_optimizer", "int3c2e_optimizer", "int2c2e_optimizer", "int2e_ip1_optimizer",
+                 "int3c2e_ip1_optimizer"):
         f = getattr(L, name)
         f.argtypes = [ctypes.POINTER(_vp), _ip, _i, _ip, _i, _dp]
         f.restype = None
@@ -171,13 +178,13 @@ def _block_len(bas, shls, sph):
     return n
 
 
-def _call(name, nsh, shls, atm, bas, env, opt=None, dims=None, out=None, sph=True):
+def _call(name, nsh, shls, atm, bas, env, opt=None, dims=None, out=None, sph=True, ncomp=1):
     atm, bas, env = _arrs(atm, bas, env)
     s = np.ascontiguousarray(shls, dtype=np.int32)
     assert s.size == nsh
     if out is None:
         n = _block_len(bas, s, sph) if dims is None else int(np.prod(dims))
-        out = np.zeros(n)
+        out = np.zeros(n * ncomp)
     d = None if dims is None else np.ascontiguousarray(dims, dtype=np.int32)
     ret = getattr(lib, name)(out.ctypes.data_as(_dp), None if d is None else d.ctypes.data_as(_ip),
                              s.ctypes.data_as(_ip), atm.ctypes.data_as(_ip), atm.shape[0],
@@ -223,6 +230,46 @@ def ao_loc(bas, sph: bool = True) -> np.ndarray:
                                                                            b.ctypes.data_as(_ip), n)
     loc[n] = (lib.CINTtot_cgto_spheric if sph else lib.CINTtot_cgto_cart)(b.ctypes.data_as(_ip), n)
     return loc
+
+
+def int2e_ip1_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
+    """(nabla i j|k l): three components, each a block in int2e_sph's layout, one after the other."""
+    return _call("int2e_ip1_sph", 4, shls, atm, bas, env, opt, dims, out, True, 3)
+
+
+def int2e_ip1_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int2e_ip1_cart", 4, shls, atm, bas, env, opt, dims, out, False, 3)
+
+
+def int3c2e_ip1_sph(shls, atm, bas, env, opt=None, dims=None, out=None):
+    """(nabla i j|k): three components, each a block in int3c2e_sph's layout."""
+    return _call("int3c2e_ip1_sph", 3, shls, atm, bas, env, opt, dims, out, True, 3)
+
+
+def int3c2e_ip1_cart(shls, atm, bas, env, opt=None, dims=None, out=None):
+    return _call("int3c2e_ip1_cart", 3, shls, atm, bas, env, opt, dims, out, False, 3)
+
+
+def ip1_eval(family: int, tuples, atm, bas, env, out_ptr: int, sph: bool = True) -> np.ndarray:
+    """First derivatives of a tuple list (family INT2E: 4 shells each, INT3C2E: 3) into the device
+    buffer at out_ptr (cintx_ip1_eval); returns each tuple's block offset."""
+    atm, bas, env = _arrs(atm, bas, env)
+    t = np.ascontiguousarray(tuples, dtype=np.int32)
+    n = t.shape[0]
+    offs = np.zeros(n, dtype=np.int64)
+    _check(lib.cintx_ip1_eval(family, ctypes.c_void_p(out_ptr), t.ctypes.data_as(_ip), n, int(sph),
+                              atm.ctypes.data_as(_ip), atm.shape[0], bas.ctypes.data_as(_ip), bas.shape[0],
+                              env.ctypes.data_as(_dp), offs.ctypes.data_as(_i64p)))
+    return offs
+
+
+def ip1_len(family: int, tuples, bas, sph: bool = True) -> int:
+    """Doubles a cintx_ip1_eval output of these tuples holds (3 components per block)."""
+    b = np.asarray(bas)
+    l, nc = b[:, 1].astype(np.int64), b[:, 3].astype(np.int64)
+    per = (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
+    t = np.asarray(tuples)
+    return int(3 * np.prod(per[t], axis=1).sum())
 
 
 def rys_roots(n: int, x: float):

@@ -150,7 +150,7 @@ bool pair_base_first(const Basis& B, int sx, int sy) {
 }
 
 // CINTset_pairdata semantics (optimizer.c:288-342) on virtual shells a (first) and b.
-void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
+void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out, int lplus) {
   const ShellInfo& A = B.sh[B.vshell[a]];
   const int ca = B.vctr[a];
   out.a = a;
@@ -192,7 +192,7 @@ void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out) {
     sp.abz = d[2];
     const double rr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     double log_rr = 1.7 - 1.5 * log(A.exps[A.nprim - 1] + Bs.exps[Bs.nprim - 1]);
-    const int lij = A.l + Bs.l;
+    const int lij = A.l + Bs.l + lplus;
     if (lij > 0) log_rr += lij * log(sqrt(rr) + 1.0);
     const double fac = sq_common * common_fac_sp(A.l) * common_fac_sp(Bs.l);
     for (int q = 0; q < Bs.nprim; ++q) {
@@ -770,7 +770,9 @@ int int2c2e_cart(double* out, int* dims, int* shls, int* atm, int natm, int* bas
 }
 
 // cintx-capi's id-dispatch surface (crates/cintx-capi/src/shim.rs:312-453) for the Coulomb ids this
-// library computes: 9 int2e_cart, 10 int2e_sph, 12 int2c2e_cart, 13 int2c2e_sph.
+// library computes: 9 int2e_cart, 10 int2e_sph, 12 int2c2e_cart, 13 int2c2e_sph, and the first
+// derivatives 18 int3c2e_ip1_cart, 19 int3c2e_ip1_sph, 35 int2e_ip1_cart, 36 int2e_ip1_sph.
+enum { F2E_IP1 = 10, F3C_IP1 = 11 };
 static int dispatch_prepare(int api, const int* dims, size_t dims_len, const int* shls, size_t shls_len,
                             const int* atm, size_t atm_len, const int* bas, size_t bas_len, const double* env,
                             size_t env_len, int* family, bool* sph, long long* nout) {
@@ -779,16 +781,21 @@ static int dispatch_prepare(int api, const int* dims, size_t dims_len, const int
     case 10: *family = F2E; *sph = true; break;
     case 12: *family = F2C; *sph = false; break;
     case 13: *family = F2C; *sph = true; break;
+    case 18: *family = F3C_IP1; *sph = false; break;
+    case 19: *family = F3C_IP1; *sph = true; break;
+    case 35: *family = F2E_IP1; *sph = false; break;
+    case 36: *family = F2E_IP1; *sph = true; break;
     default:
       set_error(CINTX_STATUS_UNSUPPORTED_API, "api id " + std::to_string(api) +
-                                                  " is not a Coulomb integral this library computes (9, 10, 12, 13)");
+                                                  " is not a Coulomb integral this library computes "
+                                                  "(9, 10, 12, 13, 18, 19, 35, 36)");
       return CINTX_STATUS_UNSUPPORTED_API;
   }
   if (!shls || !atm || !bas || !env) {
     set_error(CINTX_STATUS_NULL_POINTER, "shls, atm, bas and env must not be NULL");
     return CINTX_STATUS_NULL_POINTER;
   }
-  const int nsh = *family == F2E ? 4 : 2;
+  const int nsh = *family == F2E || *family == F2E_IP1 ? 4 : (*family == F3C_IP1 ? 3 : 2);
   const long long natm = (long long)(atm_len / ATM_SLOTS), nbas = (long long)(bas_len / BAS_SLOTS);
   if ((long long)shls_len < nsh || natm < 1 || nbas < 1) {
     set_error(CINTX_STATUS_INVALID_INPUT, "shls, atm or bas is too short");
@@ -831,7 +838,7 @@ static int dispatch_prepare(int api, const int* dims, size_t dims_len, const int
       return CINTX_STATUS_INVALID_INPUT;
     }
   }
-  *nout = n;
+  *nout = n * (*family == F2E_IP1 || *family == F3C_IP1 ? 3 : 1);  // derivatives: 3 components
   return CINTX_STATUS_SUCCESS;
 }
 
@@ -890,8 +897,18 @@ int cintrs_eval(int api, double* out, size_t out_len, const int* dims, size_t di
     return CINTX_STATUS_BUFFER_TOO_SMALL;
   }
   const int natm = (int)(atm_len / ATM_SLOTS), nbas = (int)(bas_len / BAS_SLOTS);
-  const int r = eval_call(family, sph, out, nullptr, const_cast<int*>(shls), const_cast<int*>(atm), natm,
-                          const_cast<int*>(bas), nbas, const_cast<double*>(env), const_cast<CINTOpt*>(opt));
+  int* sh = const_cast<int*>(shls);
+  int* at = const_cast<int*>(atm);
+  int* ba = const_cast<int*>(bas);
+  double* en = const_cast<double*>(env);
+  int r;
+  if (family == F2E_IP1) {
+    r = (sph ? int2e_ip1_sph : int2e_ip1_cart)(out, nullptr, sh, at, natm, ba, nbas, en, nullptr, nullptr);
+  } else if (family == F3C_IP1) {
+    r = (sph ? int3c2e_ip1_sph : int3c2e_ip1_cart)(out, nullptr, sh, at, natm, ba, nbas, en, nullptr, nullptr);
+  } else {
+    r = eval_call(family, sph, out, nullptr, sh, at, natm, ba, nbas, en, const_cast<CINTOpt*>(opt));
+  }
   if (g_err.code) return g_err.code;
   summary_out->not0 = r;
   summary_out->bytes_written = (size_t)nout * sizeof(double);

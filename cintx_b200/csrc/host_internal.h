@@ -65,7 +65,9 @@ struct PairHost {
 bool pair_base_first(const Basis& B, int sx, int sy);
 
 // Builds the screened primitive pairs of virtual shells (a, b), in that order (b < 0: unit).
-void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out);
+// lplus raises the pair's angular momentum in libcint's screening estimate (derivative integrals
+// screen with the raised ceiling li + 1, cint2e.c CINT2e_loop_nopt -> CINTset_pairdata).
+void build_pair(const Basis& B, int a, int b, double expcutoff, PairHost& out, int lplus = 0);
 
 // Device-resident state of one CINTOpt: all unordered virtual-shell pairs (u >= v) oriented by
 // angular momentum (larger l first; equal l keeps the larger index first) followed by one unit

@@ -66,6 +66,25 @@ CINTX_API int int3c2e_cart(double *out, int *dims, int *shls, int *atm, int natm
                  double *env, CINTOpt *opt, double *cache);
 CINTX_API void int3c2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
 
+/* First derivatives (nabla i j|k l) and (nabla i j|k), libcint int2e_ip1_sph / int2e_ip1_cart /
+ * int2e_ip1_optimizer (autocode/grad2.c:69-88) and int3c2e_ip1_sph / int3c2e_ip1_cart /
+ * int3c2e_ip1_optimizer (autocode/int3c2e.c:68-88); cintrs_eval api 36 / 35 and 19 / 18.  The
+ * derivative acts on the electron coordinate of the first shell; three components x, y, z, each a
+ * block in the plain layout, one after the other: out[c*blk + i + ni*(j + nj*(k + nk*l))] (with
+ * dims: out[c*dims[0]*dims[1]*... + ...]).  Return value, out == NULL and screening as int2e_sph.
+ * Compiled for l <= 3 on (i, j) and (k, l), and l <= 4 on the 3-centre auxiliary shell k; other
+ * shells set CINTX_STATUS_UNSUPPORTED_API.  The optimizer handle is accepted and not needed. */
+CINTX_API int int2e_ip1_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                            double *env, CINTOpt *opt, double *cache);
+CINTX_API int int2e_ip1_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                             double *env, CINTOpt *opt, double *cache);
+CINTX_API void int2e_ip1_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+CINTX_API int int3c2e_ip1_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                              double *env, CINTOpt *opt, double *cache);
+CINTX_API int int3c2e_ip1_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
+                               double *env, CINTOpt *opt, double *cache);
+CINTX_API void int3c2e_ip1_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, int nbas, double *env);
+
 /* Replaces libcint CINTdel_optimizer (optimizer.c:69). Sets *opt to NULL. */
 CINTX_API void CINTdel_optimizer(CINTOpt **opt);
 
@@ -154,7 +173,8 @@ typedef struct {
 } CintxEvalSummary;
 
 /* cintrs_eval / cintrs_query_workspace for the api ids 9 int2e_cart, 10 int2e_sph, 12 int2c2e_cart,
- * 13 int2c2e_sph (CintxRawApi, shim.rs:8-50; other ids return CINTX_STATUS_UNSUPPORTED_API).
+ * 13 int2c2e_sph, 18 int3c2e_ip1_cart, 19 int3c2e_ip1_sph, 35 int2e_ip1_cart, 36 int2e_ip1_sph
+ * (CintxRawApi, shim.rs:8-50; other ids return CINTX_STATUS_UNSUPPORTED_API).
  * natm = atm_len / 6 and nbas = bas_len / 8; every env slot the basis references must lie below
  * env_len; dims, when given, must equal the block's natural extents (cintx-compat layout.rs);
  * out == NULL (out_len 0) is a workspace-only call; out and cache must not alias; opt is NULL or
@@ -304,6 +324,14 @@ CINTX_API int cintx_plan_execute_host_ring(CintxPlan *plan, double *ring, int64_
                                                             int64_t n),
                                            void *user);
 CINTX_API void cintx_plan_destroy(CintxPlan *plan);
+
+/* Batched first derivatives (no libcint counterpart; the batched form of int2e_ip1 / int3c2e_ip1):
+ * family CINTX_INT2E (4 ints per tuple) or CINTX_INT3C2E (3 ints), n tuples (host), blocks back to
+ * back in list order, each 3 components of the plain block (layout of int2e_ip1_sph) into out_dev
+ * (device memory the caller sized from offsets: offsets_out, host, n entries, may be NULL).
+ * Synchronous; blocks of fully screened tuples are zero. */
+CINTX_API int cintx_ip1_eval(int family, double *out_dev, const int *shls, int64_t n, int sph, const int *atm,
+                             int natm, const int *bas, int nbas, const double *env, int64_t *offsets_out);
 
 /* ---- evaluation without device allocation ------------------------------------------------ */
 

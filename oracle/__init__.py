@@ -184,9 +184,10 @@ class RefLibcint(_Base):
 
     _batch_lib = None
 
-    def batch(self, tuples, mol, sph=True, nthreads=0):
-        """Blocks of every tuple (rows of 4, 3 or 2 shell ids: int2e, int3c2e, int2c2e) from
-        libcint, concatenated in order (_ref/libcint_batch.so, OpenMP over the tuples).
+    def batch(self, tuples, mol, sph=True, nthreads=0, ip1=False):
+        """Blocks of every tuple (rows of 4, 3 or 2 shell ids: int2e, int3c2e, int2c2e; with ip1
+        the first derivatives int2e_ip1 / int3c2e_ip1, three components per block) from libcint,
+        concatenated in order (_ref/libcint_batch.so, OpenMP over the tuples).
         Returns (values, offsets[n+1], return values)."""
         if RefLibcint._batch_lib is None:
             L = ctypes.CDLL(os.path.join(HERE, "_ref", "libcint_batch.so"))
@@ -196,12 +197,12 @@ class RefLibcint(_Base):
             L.ref_batch.restype = ctypes.c_int
             RefLibcint._batch_lib = L
         t = np.ascontiguousarray(tuples, dtype=np.int32)
-        fam = t.shape[1]
+        fam = t.shape[1] * 10 + 1 if ip1 else t.shape[1]
         atm, bas, env = self._mol(mol)
         l = bas[:, 1].astype(np.int64)
         nc = bas[:, 3].astype(np.int64)
         per = (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
-        sizes = np.prod(per[t], axis=1) if len(t) else np.zeros(0, dtype=np.int64)
+        sizes = np.prod(per[t], axis=1) * (3 if ip1 else 1) if len(t) else np.zeros(0, dtype=np.int64)
         offs = np.zeros(len(t) + 1, dtype=np.int64)
         offs[1:] = np.cumsum(sizes)
         out = np.zeros(int(offs[-1]))

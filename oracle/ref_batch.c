@@ -6,9 +6,10 @@
  * the GPU parity tests and bench.py's error record compare against; nothing in the product
  * loads it.
  *
- * family 4: int2e (4 ints per tuple), 3: int3c2e (3 ints), 2: int2c2e (2 ints); sph != 0 selects
- * the *_sph functions, else *_cart.  Block t is written at out + offs[t]; rets[t] (may be NULL)
- * receives libcint's return value.
+ * family 4: int2e (4 ints per tuple), 3: int3c2e (3 ints), 2: int2c2e (2 ints), 41: int2e_ip1
+ * (4 ints, 3 components), 31: int3c2e_ip1 (3 ints, 3 components); sph != 0 selects the *_sph
+ * functions, else *_cart.  Block t is written at out + offs[t]; rets[t] (may be NULL) receives
+ * libcint's return value.
  */
 #include <omp.h>
 #include <stdlib.h>
@@ -26,6 +27,12 @@ int int2c2e_cart(double *, int *, int *, int *, int, int *, int, double *, CINTO
 void int2e_optimizer(CINTOpt **, int *, int, int *, int, double *);
 void int3c2e_optimizer(CINTOpt **, int *, int, int *, int, double *);
 void int2c2e_optimizer(CINTOpt **, int *, int, int *, int, double *);
+int int2e_ip1_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+int int2e_ip1_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+int int3c2e_ip1_sph(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+int int3c2e_ip1_cart(double *, int *, int *, int *, int, int *, int, double *, CINTOpt *, double *);
+void int2e_ip1_optimizer(CINTOpt **, int *, int, int *, int, double *);
+void int3c2e_ip1_optimizer(CINTOpt **, int *, int, int *, int, double *);
 void CINTdel_optimizer(CINTOpt **);
 
 int ref_batch(int family, int sph, double *out, const long long *offs, const int *tuples, long long n,
@@ -42,6 +49,12 @@ int ref_batch(int family, int sph, double *out, const long long *offs, const int
         } else if (family == 2) {
                 f = sph ? int2c2e_sph : int2c2e_cart;
                 mk = int2c2e_optimizer;
+        } else if (family == 41) {
+                f = sph ? int2e_ip1_sph : int2e_ip1_cart;
+                mk = int2e_ip1_optimizer;
+        } else if (family == 31) {
+                f = sph ? int3c2e_ip1_sph : int3c2e_ip1_cart;
+                mk = int3c2e_ip1_optimizer;
         } else {
                 return 1;
         }
@@ -56,7 +69,8 @@ int ref_batch(int family, int sph, double *out, const long long *offs, const int
 #pragma omp for schedule(dynamic, 4)
                 for (long long t = 0; t < n; t++) {
                         int s[4];
-                        for (int a = 0; a < family; a++) s[a] = tuples[t * family + a];
+                        const int nsh = family > 10 ? family / 10 : family;
+                        for (int a = 0; a < nsh; a++) s[a] = tuples[t * nsh + a];
                         int need = f(NULL, NULL, s, atm, natm, bas, nbas, env, opt, NULL);
                         if (need > cap) {
                                 free(cache);

@@ -7,6 +7,9 @@
                      reference sources (oracle/_ref/libcint.so, built by oracle/Makefile) for
                      seeded samples of shell tuples of the synthetic molecules, plus a small
                      generally-contracted basis (nctr = 2) and dims / expcutoff variants.
+  libcint_ip1.npz    libcint int2e_ip1 / int3c2e_ip1 blocks (x, y, z components) for seeded tuples
+                     of the 3-atom molecule (sph, cart), the 40-atom molecule and the 3-atom
+                     molecule with its auxiliary basis (3-centre, auxiliary shells up to g).
   libcint_mol120f.npz  libcint blocks of 50 quartets from every f-containing angular-momentum
                      class of the 120-atom molecule's Schwarz-screened quartet set, each quartet
                      in a random one of its 8 index orders (libcint evaluated with each equal-l
@@ -285,10 +288,37 @@ def make_mol120():
                         class_index=cls, class_labels=np.array(labels))
 
 
+def make_ip1():
+    """libcint int2e_ip1 / int3c2e_ip1 blocks (three components each) for seeded tuples of the
+    3-atom molecule (sph and cart), the 40-atom molecule (sph) and the 3-atom molecule with its
+    auxiliary basis (3-centre, auxiliary shells up to g)."""
+    ref = RefLibcint()
+    rng = np.random.default_rng(4242)
+    d = {}
+
+    def put(name, mol, tuples, sph):
+        vals, offs, rets = ref.batch(tuples, mol, sph, ip1=True)
+        d[name + "_tuples"], d[name + "_offsets"], d[name + "_values"], d[name + "_ret"] = tuples, offs, vals, rets
+
+    w = M.water_like()
+    put("water3_int2e_ip1_sph", w, sample_tuples(rng, w.nbas, 4, 300), True)
+    put("water3_int2e_ip1_cart", w, sample_tuples(rng, w.nbas, 4, 100), False)
+    m40 = M.mol40()
+    put("mol40_int2e_ip1_sph", m40, sample_tuples(rng, m40.nbas, 4, 200), True)
+    wa = M.with_aux(w)
+    norb = w.nbas
+    t3 = np.stack([rng.integers(0, norb, 240), rng.integers(0, norb, 240), rng.integers(norb, wa.nbas, 240)],
+                  axis=1).astype(np.int32)
+    put("water3aux_int3c2e_ip1_sph", wa, t3[:160], True)
+    put("water3aux_int3c2e_ip1_cart", wa, t3[160:], False)
+    np.savez_compressed(os.path.join(HERE, "libcint_ip1.npz"), **d)
+
+
 if __name__ == "__main__":
     make_roots()
     make_integrals()
     make_mol120()
+    make_ip1()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
