@@ -74,15 +74,21 @@ struct Ip1Work {
 // Builds pairs and quartet records of n derivative tuples (nsh = 4: int2e_ip1, 3: int3c2e_ip1),
 // blocks back to back, component-major within each block.  offsets (may be NULL) receive each
 // tuple's block offset.  Returns a status code.
-int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, Ip1Work& W, int64_t* offsets) {
+// Screening follows libcint's two drivers: without an optimizer (CINT2e_loop_nopt) only the
+// differentiated pair's estimate takes the raised ceiling li + 1; with one, the optimizer's pair
+// table (CINTOpt_setij, optimizer.c:344-420) raises every pair's estimate by the derivative order
+// and keeps primitive pairs below the cut-off without its "+1" margin.
+int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, bool opt_mode, Ip1Work& W,
+              int64_t* offsets) {
   const double cutoff = nsh == 4 ? expcutoff_2e(B.env.data()) : expcutoff_3c(B.env.data());
+  const double pair_cutoff = opt_mode ? expcutoff_3c(B.env.data()) : cutoff;
   std::map<std::tuple<int, int, int>, int> pair_id;  // (a, b, derivative) -> id
   auto get_pair = [&](int a, int b, bool deriv) {
     auto key = std::make_tuple(a, b, deriv ? 1 : 0);
     auto it = pair_id.find(key);
     if (it != pair_id.end()) return it->second;
     PairHost ph;
-    build_pair(B, a, b, cutoff, ph, deriv ? 1 : 0);
+    build_pair(B, a, b, pair_cutoff, ph, deriv || (opt_mode && b >= 0) ? 1 : 0);
     if (deriv) {  // 2 a_i of each primitive pair's i primitive
       const ShellInfo& A = B.sh[B.vshell[a]];
       for (size_t k = 0; k < ph.prims.size(); ++k) ph.prims[k].q = 2.0 * A.exps[ph.pa[k]];
@@ -218,8 +224,9 @@ int ip1_launch(const Ip1Work& W, bool sph, int nsh, const Basis& B, char* dev, c
 // Evaluates n derivative tuples into out (device memory, or host memory when to_host) with the
 // thread's scratch buffers; synchronous.  *any receives libcint's return value semantics over all
 // tuples (1 if a primitive survived screening).
-int ip1_eval(int nsh, double* out, bool to_host, const int* shls, int64_t n, bool sph, const int* atm, int natm,
-             const int* bas, int nbas, const double* env, int64_t* offsets, bool* any, long long* out_doubles) {
+int ip1_eval(int nsh, double* out, bool to_host, const int* shls, int64_t n, bool sph, bool opt_mode, const int* atm,
+             int natm, const int* bas, int nbas, const double* env, int64_t* offsets, bool* any,
+             long long* out_doubles) {
   Basis B;
   int rc = load_basis(B, atm, natm, bas, nbas, env);
   if (rc) return rc;
@@ -228,7 +235,7 @@ int ip1_eval(int nsh, double* out, bool to_host, const int* shls, int64_t n, boo
     return CINTX_STATUS_UNSUPPORTED_API;
   }
   Ip1Work W;
-  if ((rc = ip1_build(B, nsh, shls, n, sph, W, offsets))) return rc;
+  if ((rc = ip1_build(B, nsh, shls, n, sph, opt_mode, W, offsets))) return rc;
   if (any) *any = W.any;
   if (out_doubles) *out_doubles = W.out_doubles;
   if (W.groups.empty()) return CINTX_STATUS_SUCCESS;
@@ -271,15 +278,16 @@ int cintx_ip1_eval(int family, double* out_dev, const int* shls, int64_t n, int 
     set_error(CINTX_STATUS_UNSUPPORTED_API, "derivative integrals exist for int2e and int3c2e");
     return CINTX_STATUS_UNSUPPORTED_API;
   }
-  return ip1_eval(family == CINTX_INT2E ? 4 : 3, out_dev, false, shls, n, sph != 0, atm, natm, bas, nbas, env,
+  return ip1_eval(family == CINTX_INT2E ? 4 : 3, out_dev, false, shls, n, sph != 0, true, atm, natm, bas, nbas, env,
                   offsets_out, nullptr, nullptr);
 }
 
 // libcint-signature derivative entry points: out == NULL returns a cache size (as libcint's drivers,
 // cint2e.c:801-818), dims places each component's block in an array of those extents, the return
-// value is 1 if a primitive survived screening (0 and zeros otherwise).
+// value is 1 if a primitive survived screening (0 and zeros otherwise), screened as libcint screens
+// with or without an optimizer (ip1_build); the optimizer's tables themselves are not needed.
 static int ip1_call(int nsh, bool sph, double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas,
-                    double* env) {
+                    double* env, bool opt_mode) {
   clear_error();
   if (!shls || !atm || !bas || !env) {
     set_error(CINTX_STATUS_NULL_POINTER, "shls, atm, bas and env must not be NULL");
@@ -300,7 +308,8 @@ static int ip1_call(int nsh, bool sph, double* out, int* dims, int* shls, int* a
   bool any = false;
   long long nd = 0;
   std::vector<double> tmp(3 * blk);
-  const int rc = ip1_eval(nsh, tmp.data(), true, shls, 1, sph, atm, natm, bas, nbas, env, nullptr, &any, &nd);
+  const int rc = ip1_eval(nsh, tmp.data(), true, shls, 1, sph, opt_mode, atm, natm, bas, nbas, env, nullptr, &any,
+                          &nd);
   if (rc) return 0;
   if (!any) std::fill(tmp.begin(), tmp.end(), 0.0);
   if (!dims) {
@@ -330,27 +339,23 @@ static int ip1_call(int nsh, bool sph, double* out, int* dims, int* shls, int* a
 
 int int2e_ip1_sph(double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas, double* env,
                   CINTOpt* opt, double* cache) {
-  (void)opt;
   (void)cache;
-  return ip1_call(4, true, out, dims, shls, atm, natm, bas, nbas, env);
+  return ip1_call(4, true, out, dims, shls, atm, natm, bas, nbas, env, opt != nullptr);
 }
 int int2e_ip1_cart(double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas, double* env,
                    CINTOpt* opt, double* cache) {
-  (void)opt;
   (void)cache;
-  return ip1_call(4, false, out, dims, shls, atm, natm, bas, nbas, env);
+  return ip1_call(4, false, out, dims, shls, atm, natm, bas, nbas, env, opt != nullptr);
 }
 int int3c2e_ip1_sph(double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas, double* env,
                     CINTOpt* opt, double* cache) {
-  (void)opt;
   (void)cache;
-  return ip1_call(3, true, out, dims, shls, atm, natm, bas, nbas, env);
+  return ip1_call(3, true, out, dims, shls, atm, natm, bas, nbas, env, opt != nullptr);
 }
 int int3c2e_ip1_cart(double* out, int* dims, int* shls, int* atm, int natm, int* bas, int nbas, double* env,
                      CINTOpt* opt, double* cache) {
-  (void)opt;
   (void)cache;
-  return ip1_call(3, false, out, dims, shls, atm, natm, bas, nbas, env);
+  return ip1_call(3, false, out, dims, shls, atm, natm, bas, nbas, env, opt != nullptr);
 }
 void int2e_ip1_optimizer(CINTOpt** opt, int* atm, int natm, int* bas, int nbas, double* env) {
   int2e_optimizer(opt, atm, natm, bas, nbas, env);

@@ -73,7 +73,9 @@ CINTX_API void int3c2e_optimizer(CINTOpt **opt, int *atm, int natm, int *bas, in
  * block in the plain layout, one after the other: out[c*blk + i + ni*(j + nj*(k + nk*l))] (with
  * dims: out[c*dims[0]*dims[1]*... + ...]).  Return value, out == NULL and screening as int2e_sph.
  * Compiled for l <= 3 on (i, j) and (k, l), and l <= 4 on the 3-centre auxiliary shell k; other
- * shells set CINTX_STATUS_UNSUPPORTED_API.  The optimizer handle is accepted and not needed. */
+ * shells set CINTX_STATUS_UNSUPPORTED_API.  Primitive screening follows libcint's driver for the
+ * call: without an optimizer only the differentiated pair's estimate takes l + 1 (CINT2e_loop_nopt);
+ * with one (its tables are not needed) every pair's does (CINTOpt_setij, optimizer.c:344). */
 CINTX_API int int2e_ip1_sph(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
                             double *env, CINTOpt *opt, double *cache);
 CINTX_API int int2e_ip1_cart(double *out, int *dims, int *shls, int *atm, int natm, int *bas, int nbas,
@@ -329,7 +331,7 @@ CINTX_API void cintx_plan_destroy(CintxPlan *plan);
  * family CINTX_INT2E (4 ints per tuple) or CINTX_INT3C2E (3 ints), n tuples (host), blocks back to
  * back in list order, each 3 components of the plain block (layout of int2e_ip1_sph) into out_dev
  * (device memory the caller sized from offsets: offsets_out, host, n entries, may be NULL).
- * Synchronous; blocks of fully screened tuples are zero. */
+ * Screened as libcint with an optimizer.  Synchronous; blocks of fully screened tuples are zero. */
 CINTX_API int cintx_ip1_eval(int family, double *out_dev, const int *shls, int64_t n, int sph, const int *atm,
                              int natm, const int *bas, int nbas, const double *env, int64_t *offsets_out);
 

@@ -34,14 +34,36 @@ def _cases():
 
 
 def test_per_call_derivatives_match_libcint_goldens(cx):
+    """The goldens come from libcint with an optimizer (its screening raises every pair's estimate by
+    the derivative order), so the per-call path runs with one too."""
     g = np.load(GOLD)
     for name, mol, fn in _cases():
         tup, offs, vals, rets = (g[name + k] for k in ("_tuples", "_offsets", "_values", "_ret"))
-        for q, t in enumerate(tup):
-            out, ret = getattr(cx, fn)(t, mol.atm, mol.bas, mol.env)
-            ref = vals[offs[q]:offs[q + 1]]
-            assert ret == rets[q], (name, t)
-            assert out.size == ref.size and close(out, ref), (name, t, np.abs(out - ref).max())
+        with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
+            for q, t in enumerate(tup):
+                out, ret = getattr(cx, fn)(t, mol.atm, mol.bas, mol.env, opt=opt)
+                ref = vals[offs[q]:offs[q + 1]]
+                assert ret == rets[q], (name, t)
+                assert out.size == ref.size and close(out, ref), (name, t, np.abs(out - ref).max())
+
+
+@pytest.mark.skipif(not RefLibcint.available(), reason="libcint from the reference sources not built")
+def test_per_call_without_optimizer_screens_like_libcint(cx):
+    """Without an optimizer libcint raises only the differentiated pair's screening estimate
+    (CINT2e_loop_nopt): return values and blocks against live libcint without one."""
+    mol = M.mol40()
+    ref = RefLibcint()
+    f = ref.lib.int2e_ip1_sph
+    rng = np.random.default_rng(77)
+    atm, bas, env = (np.ascontiguousarray(a) for a in (mol.atm, mol.bas, mol.env))
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    for t in list(rng.integers(0, mol.nbas, size=(120, 4))) + [np.array([80, 84, 27, 120])]:
+        t = np.ascontiguousarray(t, dtype=np.int32)
+        out, ret = cx.int2e_ip1_sph(t, mol.atm, mol.bas, mol.env)
+        want = np.zeros(out.size)
+        r = f(want.ctypes.data_as(dp), None, t.ctypes.data_as(ip), atm.ctypes.data_as(ip), atm.shape[0],
+              bas.ctypes.data_as(ip), bas.shape[0], env.ctypes.data_as(dp), None, None)
+        assert ret == r and close(out, want), (t, ret, r)
 
 
 def test_batched_derivatives_match_libcint_goldens(cx):
