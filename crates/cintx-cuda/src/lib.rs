@@ -216,9 +216,10 @@ impl Drop for Plan<'_> {
 }
 
 /// cintx-capi api ids this engine evaluates (`shim.rs:8-50`): int2e_cart 9, int2e_sph 10,
-/// int2c2e_cart 12, int2c2e_sph 13.
+/// int2c2e_cart 12, int2c2e_sph 13, int3c2e_ip1_cart 18, int3c2e_ip1_sph 19, int2e_ip1_cart 35,
+/// int2e_ip1_sph 36.
 pub fn handles_api(api: i32) -> bool {
-    matches!(api, 9 | 10 | 12 | 13)
+    matches!(api, 9 | 10 | 12 | 13 | 18 | 19 | 35 | 36)
 }
 
 /// For cintx-capi's `cintrs_eval`: evaluates the request here when [`handles_api`] says so and
