@@ -98,6 +98,10 @@ def parse():
                     help="quartets per class in the error_vs_libcint sample")
     ap.add_argument("--no-decomposition", action="store_true",
                     help="skip the FP64-autotuned-shapes and north-star-form comparison sweeps")
+    ap.add_argument("--shapes", default=None,
+                    help="launch shapes saved by --save-shapes: applied instead of autotuning (profiler runs, whose "
+                         "serialised launches would distort the autotuner's timings)")
+    ap.add_argument("--save-shapes", default=None, help="write the autotuned launch shapes to this JSON file")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip every comparison sweep, the plain FP64 one included (profiler runs)")
     ap.add_argument("--fp32-budget", type=float, default=FP32_BUDGET)
@@ -421,14 +425,27 @@ def timed_multi(cx, torch, items, args, stream, local, world, tune=False, steps=
     if tune:
         t0 = time.perf_counter()
         lanes = {}
+        source = "autotuned in this run"
+        if args.shapes:
+            cx.load_tuned_shapes(json.load(open(args.shapes)))
+            source = "loaded from " + os.path.basename(args.shapes)
         for (plan, mine), ring in zip(items, rings):
             if not mine:
                 continue
-            plan.autotune(ring.data_ptr(), chunk=-1, stream=stream.cuda_stream, reps=2)
+            if args.shapes:
+                plan.use_tuned_shapes()
+            else:
+                plan.autotune(ring.data_ptr(), chunk=-1, stream=stream.cuda_stream, reps=2)
             for c in mine:
                 for cl, n in zip(plan.segments(c)[0], plan.segment_lanes(c)):
                     lanes["(%d%d|%d%d)" % tuple(cl)] = int(n)
-        tuning = {"seconds": time.perf_counter() - t0, "lanes_per_quartet": dict(sorted(lanes.items()))}
+        if args.save_shapes:
+            with open(args.save_shapes, "w") as fh:
+                json.dump(cx.tuned_shapes(), fh)
+        tuning = {"seconds": time.perf_counter() - t0, "source": source,
+                  "lanes_per_quartet": dict(sorted(lanes.items())),
+                  "variant_per_class": {"(%d%d|%d%d)%s" % (r[0], r[1], r[2], r[3], " fp32" if r[4] else ""): r[5]
+                                        for r in cx.tuned_shapes()}}
     use_graph = not args.no_graph
     if use_graph:
         try:

@@ -21,7 +21,7 @@ INT2E, INT3C2E, INT2C2E = 0, 1, 2
 _API = {"CintxError", "Optimizer", "Plan", "int2c2e_cart", "int2c2e_sph", "int2e_cart", "int2e_sph",
         "int3c2e_cart", "int3c2e_sph", "lib", "launch_count", "rys_roots", "rys_t2_batch", "last_error",
         "RysNet", "ao_loc", "int2e_ip1_sph", "int2e_ip1_cart", "int3c2e_ip1_sph", "int3c2e_ip1_cart",
-        "ip1_eval", "ip1_len"}
+        "ip1_eval", "ip1_len", "tuned_shapes", "load_tuned_shapes"}
 
 
 def __getattr__(name):

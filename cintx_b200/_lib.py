@@ -111,6 +111,10 @@ def _load() -> ctypes.CDLL:
     L.cintx_plan_use_tuned_shapes.restype = _i
     L.cintx_plan_set_shape.argtypes = [_vp, _i]
     L.cintx_plan_set_shape.restype = _i
+    L.cintx_tuned_shapes_export.argtypes = [_ip, _i]
+    L.cintx_tuned_shapes_export.restype = _i
+    L.cintx_tuned_shapes_import.argtypes = [_ip, _i]
+    L.cintx_tuned_shapes_import.restype = _i
     L.cintx_plan_segment_lanes.argtypes = [_vp, _i64, _ip, _i]
     L.cintx_plan_segment_lanes.restype = _i
     L.cintx_plan_destroy.argtypes = [_vp]
@@ -270,6 +274,22 @@ def ip1_len(family: int, tuples, bas, sph: bool = True) -> int:
     per = (2 * l + 1 if sph else (l + 1) * (l + 2) // 2) * nc
     t = np.asarray(tuples)
     return int(3 * np.prod(per[t], axis=1).sum())
+
+
+def tuned_shapes() -> list:
+    """The autotuner's launch-shape choices on the current device: [li, lj, lk, ll, fp32, variant]
+    records (cintx_tuned_shapes_export), e.g. to save and reload in a later process."""
+    n = lib.cintx_tuned_shapes_export(None, 0)
+    rec = np.zeros((max(n, 1), 6), dtype=np.int32)
+    lib.cintx_tuned_shapes_export(rec.ctypes.data_as(_ip), n)
+    return rec[:n].tolist()
+
+
+def load_tuned_shapes(records) -> None:
+    """Adds saved launch-shape choices for the current device (cintx_tuned_shapes_import); plans
+    pick them up with Plan.use_tuned_shapes()."""
+    rec = np.ascontiguousarray(np.asarray(records, dtype=np.int32).reshape(-1, 6))
+    _check(lib.cintx_tuned_shapes_import(rec.ctypes.data_as(_ip), rec.shape[0]))
 
 
 def rys_roots(n: int, x: float):

@@ -1106,6 +1106,51 @@ int cintx_plan_use_tuned_shapes(CintxPlan* p) {
   return applied;
 }
 
+int cintx_tuned_shapes_export(int* records, int cap) {
+  clear_error();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tuned_mu);
+  int n = 0;
+  for (const auto& kv : g_tuned) {
+    if (std::get<0>(kv.first) != dev) continue;
+    if (records && n < cap) {
+      int* r = records + 6 * n;
+      r[0] = std::get<1>(kv.first);
+      r[1] = std::get<2>(kv.first);
+      r[2] = std::get<3>(kv.first);
+      r[3] = std::get<4>(kv.first);
+      r[4] = std::get<5>(kv.first);
+      r[5] = kv.second;
+    }
+    ++n;
+  }
+  return n;
+}
+
+int cintx_tuned_shapes_import(const int* records, int n) {
+  clear_error();
+  if (n < 0 || (n > 0 && !records)) {
+    set_error(CINTX_STATUS_NULL_POINTER, "records must hold n entries");
+    return CINTX_STATUS_NULL_POINTER;
+  }
+  for (int i = 0; i < n; ++i) {
+    const int* r = records + 6 * i;
+    if (r[0] < 0 || r[0] > CINTX_LMAX || r[1] < 0 || r[2] < 0 || r[3] < 0 || r[5] < 0 || r[5] >= kLaunchVariants) {
+      set_error(CINTX_STATUS_INVALID_INPUT, "tuned-shape record " + std::to_string(i) + " is out of range");
+      return CINTX_STATUS_INVALID_INPUT;
+    }
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tuned_mu);
+  for (int i = 0; i < n; ++i) {
+    const int* r = records + 6 * i;
+    g_tuned[std::make_tuple(dev, r[0], r[1], r[2], r[3], r[4] ? 1 : 0)] = r[5];
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
 int cintx_plan_set_shape(CintxPlan* p, int variant) {
   clear_error();
   if (!p) {

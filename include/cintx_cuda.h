@@ -303,6 +303,13 @@ CINTX_API int cintx_plan_autotune(CintxPlan *plan, int64_t chunk, double *out_de
  * (any plan) to this plan's matching classes; returns the number of segments changed (or -1).
  * A graph captured earlier is released when anything changed. */
 CINTX_API int cintx_plan_use_tuned_shapes(CintxPlan *plan);
+/* The launch shapes the autotuner chose in this process on the current device, as records of six
+ * ints (li, lj, lk, ll, fp32, variant): cintx_tuned_shapes_export writes up to cap records and
+ * returns how many there are; cintx_tuned_shapes_import adds n records (e.g. saved by an earlier
+ * process on the same kind of GPU) to the current device's choices, for cintx_plan_use_tuned_shapes
+ * to apply without tuning again.  Import returns a status code. */
+CINTX_API int cintx_tuned_shapes_export(int *records, int cap);
+CINTX_API int cintx_tuned_shapes_import(const int *records, int n);
 /* Sets the launch-shape variant (0..9) of every segment, for tests and tuning scripts; a class
  * that the variant does not apply to runs its default shape.  Returns the number of segments
  * changed (or -1).  A graph captured earlier is released when anything changed. */

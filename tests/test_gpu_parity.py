@@ -234,6 +234,13 @@ def test_autotuned_launch_shapes_give_the_same_integrals(cx):
         assert other.use_tuned_shapes() > 0
         assert all(np.array_equal(other.segment_lanes(c), tuned_lanes[c]) for c in range(st.nchunks))
         other.close()
+        # the choices export as records and import back (what a later process loads from a file)
+        recs = cx.tuned_shapes()
+        assert len(recs) > 0 and all(len(r) == 6 and 0 <= r[5] < 10 for r in recs)
+        cx.load_tuned_shapes(recs)
+        assert cx.tuned_shapes() == recs
+        with pytest.raises(cx.CintxError):
+            cx.load_tuned_shapes([[0, 0, 0, 0, 0, 99]])
         plan.close()
 
 
