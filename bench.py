@@ -42,7 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from cintx_b200 import molecules as M  # noqa: E402
-from cintx_b200.sharding import assign_chunks, chunks_of, max_over_ranks  # noqa: E402
+from cintx_b200.sharding import assign_chunks, chunk_doubles_for, chunks_of, max_over_ranks  # noqa: E402
 
 WORKLOADS = {
     "mol40_spd": (M.mol40, "40 seeded atoms in a 14-bohr cube, 60% light (2s,1p) / 40% heavy "
@@ -88,7 +88,9 @@ def parse():
     ap.add_argument("--workload", default="mol120_spdf",
                     choices=sorted(WORKLOADS) + sorted(DF_WORKLOADS) + ["mol20_g_learned"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--chunk-doubles", type=int, default=1 << 30)
+    ap.add_argument("--chunk-doubles", type=int, default=1 << 30,
+                    help="largest chunk of the device sweep (output doubles); with N > 1 ranks chunks shrink "
+                         "so that every rank gets about four")
     ap.add_argument("--branches", type=int, default=4)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--form", default="tuned", choices=["tuned", "plain"])
@@ -763,6 +765,10 @@ def our_arm(args):
         return chunks_of(assign_chunks([float(p.segments(c)[2].sum()) for c in range(p.stats.nchunks)], world), rank)
 
     plan = make_plan(opt, "tuned" if tuned else "plain", args.chunk_doubles)
+    cd = chunk_doubles_for(plan.stats.nintegrals, world, args.chunk_doubles)
+    if cd != args.chunk_doubles:  # N > 1: about four chunks per rank for the longest-first split
+        args.chunk_doubles = cd
+        plan = make_plan(opt, "tuned" if tuned else "plain", cd)
     st = plan.stats
     nchunks = st.nchunks
     mine = shard(plan)
@@ -985,6 +991,10 @@ def df_arm(args):
 
     opt = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
     p3, p2 = make(opt)
+    cd = chunk_doubles_for(p3.stats.nintegrals, world, args.chunk_doubles)
+    if cd != args.chunk_doubles:  # N > 1: about four chunks per rank for the longest-first split
+        args.chunk_doubles = cd
+        p3, p2 = make(opt)
     s3, s2 = p3.stats, p2.stats
     mine3 = chunks_of(assign_chunks([float(p3.segments(c)[2].sum()) for c in range(s3.nchunks)], world), rank)
     mine2 = [0] if rank == 0 else []

@@ -27,6 +27,16 @@ def chunks_of(owner, rank: int):
     return [c for c, r in enumerate(owner) if r == rank]
 
 
+def chunk_doubles_for(nintegrals: int, world: int, cap: int, per_rank: int = 4, floor: int = 1 << 22) -> int:
+    """Chunk size (output doubles) for a sweep of `nintegrals` split over `world` ranks: `cap` on
+    one rank (fewest launches), else small enough that every rank gets about `per_rank` chunks, so
+    the longest-first assignment has items to balance; never below `floor`."""
+    if world <= 1 or nintegrals <= 0:
+        return cap
+    want = -(-int(nintegrals) // (per_rank * world))
+    return int(min(cap, max(floor, want)))
+
+
 def plan_digest(plan, world: int) -> dict:
     """What a rank needs to agree on with the others before it takes its share of a sweep: the
     plan's chunk sizes, each chunk's kernel-class segments and a hash of its quartet list, and the

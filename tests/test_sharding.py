@@ -62,3 +62,15 @@ def test_two_gloo_ranks_agree_and_reduce_max():
     assert g0 == g1  # both ranks see the same assignment
     assert sorted(g0[0] + g0[1]) == list(range(len(costs))) and not set(g0[0]) & set(g0[1])
     assert res[0][2] == res[1][2] == 11.0  # max of the per-rank times
+
+
+def test_chunk_size_per_world():
+    from cintx_b200.sharding import chunk_doubles_for
+    nint = 6_127_704_505  # mol120_spdf's sweep
+    cap = 1 << 30
+    assert chunk_doubles_for(nint, 1, cap) == cap
+    for world in (2, 4, 8):
+        cd = chunk_doubles_for(nint, world, cap)
+        assert cd <= cap
+        assert -(-nint // cd) >= 4 * world  # every rank gets about four chunks to balance
+    assert chunk_doubles_for(1000, 8, cap) == 1 << 22  # tiny sweeps keep a floor
