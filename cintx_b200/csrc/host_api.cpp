@@ -11,9 +11,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cintx_cuda.h"
@@ -39,6 +42,21 @@ void set_error(int code, const std::string& msg) {
 void clear_error() {
   g_err.code = 0;
   g_err.msg.clear();
+}
+
+static double wall_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+PhaseLog::PhaseLog(const char* what_) : what(what_), t(0) {
+  const char* e = getenv("CINTX_PLAN_LOG");
+  on = e && e[0] && e[0] != '0';
+  if (on) t = wall_ms();
+}
+void PhaseLog::mark(const char* phase) {
+  if (!on) return;
+  const double now = wall_ms();
+  fprintf(stderr, "cintx %s: %s %.2f ms\n", what, phase, now - t);
+  t = now;
 }
 
 // ---------------------------------------------------------------- basis
@@ -360,6 +378,7 @@ static void free_opt_device(Opt* o) {
 }
 
 int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const double* env, int npair_shells) {
+  PhaseLog plog("optimizer");
   int rc = load_basis(o->basis, atm, natm, bas, nbas, env);
   if (rc) return rc;
   if (npair_shells > nbas) {
@@ -385,27 +404,66 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
   o->pair_min_cce.assign(ntot, 0);
   o->h_prim_a.clear();
   o->h_prim_b.clear();
-  PairHost ph;
-  for (int u = 0; u < npv; ++u) {
-    for (int v = 0; v <= u; ++v) {
-      // recurrence centre first (pair_base_first; contractions of one shell: larger index first)
-      const bool uf = pair_base_first(B, B.vshell[u], B.vshell[v]);
-      const int a = uf ? u : v, b = uf ? v : u;
-      build_pair(B, a, b, o->build_cutoff, ph);
-      const int id = pair_index(u, v);
-      ph.sp.prim_off = (int)prims.size();
-      sps[id] = ph.sp;
-      prims.insert(prims.end(), ph.prims.begin(), ph.prims.end());
-      o->h_prim_a.insert(o->h_prim_a.end(), ph.pa.begin(), ph.pa.end());
-      o->h_prim_b.insert(o->h_prim_b.end(), ph.pb.begin(), ph.pb.end());
-      o->pair_a[id] = a;
-      o->pair_b[id] = b;
-      o->pair_la[id] = ph.la;
-      o->pair_lb[id] = ph.lb;
-      o->pair_nprim[id] = ph.sp.nprim;
-      o->pair_min_cce[id] = ph.min_cce;
+  // Pairs of rows u in [u0, u1) have the contiguous ids [pair_index(u0, 0), pair_index(u1, 0)), so
+  // host threads fill row ranges of about equal pair counts, each into its own primitive lists,
+  // which are then joined in row order (the order of one serial pass).
+  {
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int nt = npv >= 64 ? nthr : 1;
+    std::vector<int> ubound(nt + 1, npv);
+    ubound[0] = 0;
+    for (int t = 1; t < nt; ++t) {
+      const double target = (double)o->npairs * t / nt;  // rows below u hold u(u+1)/2 pairs
+      ubound[t] = std::max(ubound[t - 1], std::min(npv, (int)ceil((sqrt(8.0 * target + 1.0) - 1.0) / 2.0)));
+    }
+    struct Part {
+      std::vector<PrimPair> prims;
+      std::vector<int> pa, pb;
+    };
+    std::vector<Part> parts(nt);
+    auto work = [&](int t) {
+      PairHost ph;
+      Part& P = parts[t];
+      for (int u = ubound[t]; u < ubound[t + 1]; ++u) {
+        for (int v = 0; v <= u; ++v) {
+          // recurrence centre first (pair_base_first; contractions of one shell: larger index first)
+          const bool uf = pair_base_first(B, B.vshell[u], B.vshell[v]);
+          const int a = uf ? u : v, b = uf ? v : u;
+          build_pair(B, a, b, o->build_cutoff, ph);
+          const int id = pair_index(u, v);
+          ph.sp.prim_off = (int)P.prims.size();  // part-relative; shifted below
+          sps[id] = ph.sp;
+          P.prims.insert(P.prims.end(), ph.prims.begin(), ph.prims.end());
+          P.pa.insert(P.pa.end(), ph.pa.begin(), ph.pa.end());
+          P.pb.insert(P.pb.end(), ph.pb.begin(), ph.pb.end());
+          o->pair_a[id] = a;
+          o->pair_b[id] = b;
+          o->pair_la[id] = ph.la;
+          o->pair_lb[id] = ph.lb;
+          o->pair_nprim[id] = ph.sp.nprim;
+          o->pair_min_cce[id] = ph.min_cce;
+        }
+      }
+    };
+    if (nt == 1) {
+      work(0);
+    } else {
+      std::vector<std::thread> th;
+      for (int t = 0; t < nt; ++t) th.emplace_back(work, t);
+      for (auto& x : th) x.join();
+    }
+    long long base = 0;
+    for (int t = 0; t < nt; ++t) {
+      const int id0 = pair_index(ubound[t], 0);
+      const int id1 = ubound[t + 1] >= npv ? o->npairs : pair_index(ubound[t + 1], 0);
+      for (int id = id0; id < id1; ++id) sps[id].prim_off += (int)base;
+      base += (long long)parts[t].prims.size();
+      prims.insert(prims.end(), parts[t].prims.begin(), parts[t].prims.end());
+      o->h_prim_a.insert(o->h_prim_a.end(), parts[t].pa.begin(), parts[t].pa.end());
+      o->h_prim_b.insert(o->h_prim_b.end(), parts[t].pb.begin(), parts[t].pb.end());
     }
   }
+  PairHost ph;
   for (int v = 0; v < nv; ++v) {
     build_pair(B, v, -1, o->build_cutoff, ph);
     const int id = o->npairs + v;
@@ -421,6 +479,7 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
     o->pair_nprim[id] = ph.sp.nprim;
     o->pair_min_cce[id] = ph.min_cce;
   }
+  plog.mark("basis + pair tables (host)");
   if ((int64_t)prims.size() > 2000000000LL) {
     set_error(CINTX_STATUS_MEMORY_LIMIT_EXCEEDED, "too many primitive pairs");
     return CINTX_STATUS_MEMORY_LIMIT_EXCEEDED;
@@ -443,6 +502,7 @@ int build_opt(Opt* o, const int* atm, int natm, const int* bas, int nbas, const 
     set_error(CINTX_STATUS_EXECUTION_FAILED, "upload of pair tables failed");
     return CINTX_STATUS_EXECUTION_FAILED;
   }
+  plog.mark("upload");
   return CINTX_STATUS_SUCCESS;
 }
 

@@ -21,6 +21,16 @@ constexpr int PTR_EXPCUTOFF = 0, PTR_RANGE_OMEGA = 8;
 void set_error(int code, const std::string& msg);
 void clear_error();
 
+// Host-phase timer of the optimizer and plan builders: with CINTX_PLAN_LOG=1 in the environment,
+// mark() prints the wall time since the previous mark (or construction) to stderr.
+struct PhaseLog {
+  explicit PhaseLog(const char* what);
+  void mark(const char* phase);
+  bool on;
+  const char* what;
+  double t;
+};
+
 // One contracted shell of the caller's basis.
 struct ShellInfo {
   int l, nprim, nctr, atom;
@@ -166,6 +176,6 @@ cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, 
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
 // Distinct launch shape of a variant (lanes and register cap), for telling variants apart.
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-constexpr int kLaunchVariants = 10;
+constexpr int kLaunchVariants = 12;
 
 }  // namespace cintx

@@ -13,10 +13,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -117,6 +119,7 @@ struct CintxPlan {
   std::vector<Tile> tiles;
   QuartetRec* d_recs = nullptr;    // explicit: all records; screened: one chunk's records
   long long rec_capacity = 0;
+  char* d_tile_pool = nullptr;     // screened: every tile's rows, cols, prefix and colstart arrays
   std::vector<QuartetRec> h_recs;  // explicit plans keep a host copy for chunk_quartets
   std::vector<int> h_tuples;       // explicit: requested tuples (4 per record, -1 for unit)
   CintxPlanStats stats{};
@@ -150,11 +153,9 @@ namespace {
 void free_plan_device(CintxPlan* p) {
   if (p->d_recs) cudaFree(p->d_recs);
   p->d_recs = nullptr;
+  if (p->d_tile_pool) cudaFree(p->d_tile_pool);  // the tiles' arrays live in it
+  p->d_tile_pool = nullptr;
   for (Tile& t : p->tiles) {
-    if (t.d_rows) cudaFree(t.d_rows);
-    if (t.d_cols) cudaFree(t.d_cols);
-    if (t.d_prefix) cudaFree(t.d_prefix);
-    if (t.d_colstart) cudaFree(t.d_colstart);
     t.d_colstart = nullptr;
     t.d_rows = t.d_cols = nullptr;
     t.d_prefix = nullptr;
@@ -734,7 +735,6 @@ int cintx_plan_use_learned_roots(CintxPlan* p, const float* params, int64_t* nfa
 static bool ao_maps(CintxPlan* p, const std::vector<int>& aoloc) {
   if (p->d_psh) return true;
   const Opt* o = p->opt;
-  const Basis& B = o->basis;
   // block axes 0 and 1 of a pair: its shells in reported order (the layout screened plans write)
   std::vector<int2> psh(o->npairs);
   for (int id = 0; id < o->npairs; ++id) psh[id] = reported_shells(o, id);
@@ -939,7 +939,6 @@ int cintx_plan_chunk_segments(const CintxPlan* p, int64_t chunk, int* cls, int64
 int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int* quartets) {
   if (!p || !quartets || n < 0) return CINTX_STATUS_NULL_POINTER;
   const Opt* o = p->opt;
-  const Basis& B = o->basis;
   uint64_t st = seed;
   auto next = [&]() {  // splitmix64
     st += 0x9E3779B97F4A7C15ull;
@@ -1305,9 +1304,27 @@ namespace cintx {
 // exponent screening) gives every needed primitive diagonal block (ab|ab) in cartesian form on
 // the device; q_ab = |c_a c_b| sqrt(max|(ab|ab)|) then bounds every cartesian primitive integral
 // of a quartet, |c_a c_b c_c c_d (ab|cd)| <= q_ab q_cd (Cauchy-Schwarz for the Coulomb metric).
+// Pieces of the calling thread's device scratch (grown to fit, kept between calls), one per
+// requested byte size, each 256-byte aligned.  Valid until the thread's next scratch request; the
+// one-shot passes below use them instead of allocating and freeing device memory on every plan.
+static int scratch_pieces(ThreadScratch** ts, const std::vector<size_t>& sizes, std::vector<char*>& out) {
+  size_t total = 0;
+  for (size_t b : sizes) total += (b + 255) & ~(size_t)255;
+  int rc = thread_scratch(ts, std::max<size_t>(total, 256), 0);
+  if (rc) return rc;
+  out.clear();
+  char* p = static_cast<char*>((*ts)->dbuf);
+  for (size_t b : sizes) {
+    out.push_back(p);
+    p += (b + 255) & ~(size_t)255;
+  }
+  return CINTX_STATUS_SUCCESS;
+}
+
 int compute_prim_schwarz(Opt* o) {
   std::lock_guard<std::mutex> lk(o->mu);
   if (o->prim_schwarz) return CINTX_STATUS_SUCCESS;
+  PhaseLog plog("primitive Schwarz");
   const Basis& B = o->basis;
   DeviceState* ds;
   ThreadScratch* ts;
@@ -1351,16 +1368,16 @@ int compute_prim_schwarz(Opt* o) {
         len.push_back(n);
       }
     }
-    ShellPair* d_tp = nullptr;
-    QuartetRec* d_recs = nullptr;
-    double* d_out = nullptr;
-    long long* d_len = nullptr;
-    double* d_q = nullptr;
-    bool ok = cudaMalloc(&d_tp, sizeof(ShellPair) * nk) == cudaSuccess &&
-              cudaMalloc(&d_recs, sizeof(QuartetRec) * recs.size()) == cudaSuccess &&
-              cudaMalloc(&d_out, sizeof(double) * std::max(tot, 1LL)) == cudaSuccess &&
-              cudaMalloc(&d_len, sizeof(long long) * len.size()) == cudaSuccess &&
-              cudaMalloc(&d_q, sizeof(double) * recs.size()) == cudaSuccess;
+    plog.mark("records (host)");
+    std::vector<char*> pc;
+    bool ok = scratch_pieces(&ts, {sizeof(ShellPair) * nk, sizeof(QuartetRec) * recs.size(),
+                                   sizeof(double) * std::max(tot, 1LL), sizeof(long long) * len.size(),
+                                   sizeof(double) * recs.size()}, pc) == CINTX_STATUS_SUCCESS;
+    ShellPair* d_tp = ok ? reinterpret_cast<ShellPair*>(pc[0]) : nullptr;
+    QuartetRec* d_recs = ok ? reinterpret_cast<QuartetRec*>(pc[1]) : nullptr;
+    double* d_out = ok ? reinterpret_cast<double*>(pc[2]) : nullptr;
+    long long* d_len = ok ? reinterpret_cast<long long*>(pc[3]) : nullptr;
+    double* d_q = ok ? reinterpret_cast<double*>(pc[4]) : nullptr;
     if (ok) {
       cudaMemcpyAsync(d_tp, tp.data(), sizeof(ShellPair) * nk, cudaMemcpyHostToDevice, ts->stream);
       cudaMemcpyAsync(d_recs, recs.data(), sizeof(QuartetRec) * recs.size(), cudaMemcpyHostToDevice, ts->stream);
@@ -1390,11 +1407,7 @@ int compute_prim_schwarz(Opt* o) {
       if (ok)
         for (size_t i = 0; i < recs.size(); ++i) qk[recs[i].pij] = q[i];
     }
-    cudaFree(d_tp);
-    cudaFree(d_recs);
-    cudaFree(d_out);
-    cudaFree(d_len);
-    cudaFree(d_q);
+    plog.mark("device pass");
     if (!ok) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, "primitive Schwarz pass failed");
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -1403,7 +1416,8 @@ int compute_prim_schwarz(Opt* o) {
   // q per stored primitive pair, sorted by decreasing q within each shell pair
   o->pair_qp.assign(o->npairs + B.nvirt, 0.0);
   o->pair_amp.assign(o->npairs + B.nvirt, 1.0);
-  for (int id = 0; id < o->npairs; ++id) {
+  // each pair writes only its own primitive range and entries: blocks of pairs run on host threads
+  auto sort_pair = [&](int id) {
     const int a = o->pair_a[id], b = o->pair_b[id];
     const ShellInfo& SA = B.sh[B.vshell[a]];
     const ShellInfo& SB = B.sh[B.vshell[b]];
@@ -1441,7 +1455,21 @@ int compute_prim_schwarz(Opt* o) {
       o->h_prim_b[k0 + i] = pb[i];
     }
     o->pair_qp[id] = sum;
+  };
+  {
+    const int nblk = (o->npairs + 4095) / 4096;
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+      for (int j; (j = next.fetch_add(1)) < nblk;)
+        for (int id = j * 4096; id < std::min(o->npairs, (j + 1) * 4096); ++id) sort_pair(id);
+    };
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int i = 1; i < std::min(nthr, nblk); ++i) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
   }
+  plog.mark("sort primitive pairs (host)");
   if (!o->h_prims.empty() &&
       cudaMemcpy(o->d_prims, o->h_prims.data(), sizeof(PrimPair) * o->h_prims.size(), cudaMemcpyHostToDevice) !=
           cudaSuccess) {
@@ -1449,6 +1477,100 @@ int compute_prim_schwarz(Opt* o) {
     return CINTX_STATUS_EXECUTION_FAILED;
   }
   o->prim_schwarz = true;
+  plog.mark("upload");
+  return CINTX_STATUS_SUCCESS;
+}
+
+// Contracted Schwarz factors Q_ij = sqrt(max |(ij|ij)|) of every stored pair, from its spherical
+// diagonal block: the class kernels evaluate the blocks into the thread's device scratch (classes
+// (la lb|la lb), batches of at most 2^25 doubles), block_absmax_sqrt_kernel reduces each block to
+// its factor, and only the factors come back to the host.  Same kernels, launch shapes and records
+// as an explicit plan of the tuples (a b a b), so the factors are those of that plan bit for bit.
+int diag_schwarz_2e(Opt* o, double ecut, std::vector<double>& Q) {
+  const int np = o->npairs;
+  Q.assign(np, 0.0);
+  DeviceState* ds;
+  ThreadScratch* ts;
+  int rc;
+  if ((rc = device_state(&ds)) || (rc = thread_scratch(&ts, 0, 0))) return rc;
+  std::map<std::pair<int, int>, std::vector<int>> cls;  // (la, lb) -> pair ids
+  for (int id = 0; id < np; ++id)
+    if (o->pair_nprim[id] > 0) cls[std::make_pair(o->pair_la[id], o->pair_lb[id])].push_back(id);
+  const long long cap = 1LL << 25;  // doubles of diagonal blocks per batch
+  std::vector<QuartetRec> recs;
+  std::vector<long long> len;
+  std::vector<int> ids;
+  std::vector<std::pair<int, int>> seg_cls;  // class of each segment of the batch
+  std::vector<long long> seg_end;            // record end of each segment
+  bool ok = true;
+  auto flush = [&](long long tot) {
+    const long long n = (long long)recs.size();
+    if (n > 0 && ok) {
+      std::vector<char*> pc;
+      ok = scratch_pieces(&ts, {sizeof(QuartetRec) * n, sizeof(long long) * n, sizeof(double) * n,
+                                sizeof(double) * std::max(tot, 1LL)}, pc) == CINTX_STATUS_SUCCESS;
+      if (ok) {
+        QuartetRec* d_recs = reinterpret_cast<QuartetRec*>(pc[0]);
+        long long* d_len = reinterpret_cast<long long*>(pc[1]);
+        double* d_q = reinterpret_cast<double*>(pc[2]);
+        double* d_out = reinterpret_cast<double*>(pc[3]);
+        cudaMemcpyAsync(d_recs, recs.data(), sizeof(QuartetRec) * n, cudaMemcpyHostToDevice, ts->stream);
+        cudaMemcpyAsync(d_len, len.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, ts->stream);
+        long long r0 = 0;
+        for (size_t g = 0; g < seg_cls.size() && ok; ++g) {
+          const int la = seg_cls[g].first, lb = seg_cls[g].second;
+          const OutStrides st = canonical_strides(la, lb, la, true);
+          for (long long q0 = r0; q0 < seg_end[g] && ok; q0 += 1LL << 30) {
+            const int nr = (int)std::min<long long>(seg_end[g] - q0, 1LL << 30);
+            ok = launch_class(la, lb, la, lb, true, d_recs + q0, nr, o->d_pairs, o->d_prims, d_out, st, ecut,
+                              ds->rys, ts->stream, false, 0.0, 0, nullptr, nullptr) == cudaSuccess;
+            ts->launches++;
+          }
+          r0 = seg_end[g];
+        }
+        ok = ok && launch_block_absmax_sqrt(d_recs, n, d_out, d_len, d_q, ts->stream) == cudaSuccess;
+        std::vector<double> q(n);
+        ok = ok &&
+             cudaMemcpyAsync(q.data(), d_q, sizeof(double) * n, cudaMemcpyDeviceToHost, ts->stream) == cudaSuccess &&
+             cudaStreamSynchronize(ts->stream) == cudaSuccess;
+        if (ok)
+          for (long long i = 0; i < n; ++i) Q[ids[i]] = q[i];
+      }
+    }
+    recs.clear();
+    len.clear();
+    ids.clear();
+    seg_cls.clear();
+    seg_end.clear();
+  };
+  long long tot = 0;
+  for (auto& kv : cls) {
+    const int la = kv.first.first, lb = kv.first.second;
+    const long long n = (long long)nsph_or_cart(la, true) * nsph_or_cart(lb, true) * nsph_or_cart(la, true) *
+                        nsph_or_cart(lb, true);
+    for (int id : kv.second) {
+      if (tot + n > cap && !recs.empty()) {  // close the batch: its last segment is this class so far
+        seg_cls.push_back(kv.first);
+        seg_end.push_back((long long)recs.size());
+        flush(tot);
+        tot = 0;
+      }
+      QuartetRec r;
+      r.pij = r.pkl = id;
+      r.out = tot;
+      recs.push_back(r);
+      len.push_back(n);
+      ids.push_back(id);
+      tot += n;
+    }
+    seg_cls.push_back(kv.first);
+    seg_end.push_back((long long)recs.size());
+  }
+  flush(tot);
+  if (!ok) {
+    set_error(CINTX_STATUS_EXECUTION_FAILED, "diagonal Schwarz pass failed");
+    return CINTX_STATUS_EXECUTION_FAILED;
+  }
   return CINTX_STATUS_SUCCESS;
 }
 
@@ -1585,20 +1707,37 @@ static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk,
   p->rec_capacity = max_recs;
   bool ok = true;
   if (max_recs > 0) ok = cudaMalloc(&p->d_recs, sizeof(QuartetRec) * max_recs) == cudaSuccess;
-  for (Tile& t : p->tiles) {
-    if (!ok) break;
-    ok = cudaMalloc(&t.d_rows, sizeof(int) * t.rows.size()) == cudaSuccess &&
-         cudaMalloc(&t.d_cols, sizeof(int) * t.cols.size()) == cudaSuccess &&
-         cudaMalloc(&t.d_prefix, sizeof(long long) * t.row_prefix.size()) == cudaSuccess;
-    if (ok && !t.colstart.empty()) {
-      ok = cudaMalloc(&t.d_colstart, sizeof(int) * t.colstart.size()) == cudaSuccess;
-      if (ok) cudaMemcpy(t.d_colstart, t.colstart.data(), sizeof(int) * t.colstart.size(), cudaMemcpyHostToDevice);
+  // every tile's arrays in one device allocation and one copy (256-byte aligned slices)
+  if (ok && !p->tiles.empty()) {
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t total = 0;
+    for (const Tile& t : p->tiles)
+      total += align(sizeof(int) * t.rows.size()) + align(sizeof(int) * t.cols.size()) +
+               align(sizeof(long long) * t.row_prefix.size()) + align(sizeof(int) * t.colstart.size());
+    std::vector<char> img(std::max<size_t>(total, 1));
+    std::vector<size_t> at;  // slice offsets: rows, cols, prefix, colstart of each tile
+    size_t pos = 0;
+    auto put = [&](const void* src, size_t bytes) {
+      at.push_back(pos);
+      if (bytes) memcpy(img.data() + pos, src, bytes);
+      pos += align(bytes);
+    };
+    for (const Tile& t : p->tiles) {
+      put(t.rows.data(), sizeof(int) * t.rows.size());
+      put(t.cols.data(), sizeof(int) * t.cols.size());
+      put(t.row_prefix.data(), sizeof(long long) * t.row_prefix.size());
+      put(t.colstart.data(), sizeof(int) * t.colstart.size());
     }
-    if (ok) {
-      cudaMemcpy(t.d_rows, t.rows.data(), sizeof(int) * t.rows.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(t.d_cols, t.cols.data(), sizeof(int) * t.cols.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(t.d_prefix, t.row_prefix.data(), sizeof(long long) * t.row_prefix.size(), cudaMemcpyHostToDevice);
-    }
+    ok = cudaMalloc(&p->d_tile_pool, std::max<size_t>(total, 256)) == cudaSuccess;
+    if (ok) ok = cudaMemcpy(p->d_tile_pool, img.data(), total, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok)
+      for (size_t i = 0; i < p->tiles.size(); ++i) {
+        Tile& t = p->tiles[i];
+        t.d_rows = reinterpret_cast<int*>(p->d_tile_pool + at[4 * i]);
+        t.d_cols = reinterpret_cast<int*>(p->d_tile_pool + at[4 * i + 1]);
+        t.d_prefix = reinterpret_cast<long long*>(p->d_tile_pool + at[4 * i + 2]);
+        t.d_colstart = t.colstart.empty() ? nullptr : reinterpret_cast<int*>(p->d_tile_pool + at[4 * i + 3]);
+      }
   }
   // merge each chunk's tile pieces into one segment per kernel class (records of a class are
   // contiguous; each record carries its chunk-relative output offset)
@@ -1719,33 +1858,13 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
     int rc0 = compute_prim_schwarz(o);
     if (rc0) return rc0;
   }
+  PhaseLog plog("int2e plan");
   const int np = o->npairs;
-  const int nb = B.nbas;
-  // 1. Schwarz factors from the diagonal (ij|ij) blocks, cartesian-free (sph) evaluation
-  std::vector<int> diag((size_t)np * 4);
-  for (int u = 0; u < nb; ++u)
-    for (int v = 0; v <= u; ++v) {
-      const int id = pair_index(u, v);
-      const int a = o->pair_a[id], b = o->pair_b[id];
-      int* d = &diag[(size_t)id * 4];
-      d[0] = a; d[1] = b; d[2] = a; d[3] = b;
-    }
-  std::vector<int64_t> doff(np);
-  CintxPlan* dp = nullptr;
-  int rc = cintx_plan_shells(&dp, optp, CINTX_INT2E, diag.data(), np, 1, doff.data());
+  // 1. Schwarz factors from the diagonal (ij|ij) blocks, spherical, reduced on the device
+  std::vector<double> Q;
+  int rc = diag_schwarz_2e(o, expcutoff_2e(B.env.data()), Q);
   if (rc) return rc;
-  std::vector<double> dout(std::max<int64_t>(dp->stats.nintegrals, 1));
-  rc = cintx_plan_execute_host(dp, 0, dout.data());
-  const long long dn = dp->stats.nintegrals;
-  cintx_plan_destroy(dp);
-  if (rc) return rc;
-  std::vector<double> Q(np, 0.0);
-  for (int id = 0; id < np; ++id) {
-    const long long e0 = doff[id], e1 = id + 1 < np ? doff[id + 1] : dn;
-    double m = 0;
-    for (long long e = e0; e < e1; ++e) m = std::max(m, fabs(dout[e]));
-    Q[id] = sqrt(m);
-  }
+  plog.mark("diagonal Schwarz pass");
   // 2. pair types (la, lb, nprim_a, nprim_b), sorted pairs by decreasing Q
   std::map<std::tuple<int, int, int, int>, std::vector<int>> types;
   double qmax = 0;
@@ -1770,86 +1889,113 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
   const double ecut = expcutoff_2e(B.env.data());
   long long nq_total = 0, nint_total = 0, nq_fp32 = 0;
   const int nt = (int)tlist.size();
-  // tiles A >= B in type order (types are ordered by (la, lb, ...), so classes are valid)
-  for (int A = 0; A < nt; ++A) {
-    for (int Bt = 0; Bt <= A; ++Bt) {
-      Tile t;
-      t.typeA = A;
-      t.typeB = Bt;
-      t.li = std::get<0>(tkeys[A]);
-      t.lj = std::get<1>(tkeys[A]);
-      t.lk = std::get<0>(tkeys[Bt]);
-      t.ll = std::get<1>(tkeys[Bt]);
-      t.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
-      // equal-l pairs are reported (other, centre): their two axes trade strides
-      if (t.li == t.lj) std::swap(t.st.s0, t.st.s1);
-      if (t.lk == t.ll) std::swap(t.st.s2, t.st.s3);
-      const std::vector<int>& rows = tlist[A];
-      const std::vector<int>& cols = tlist[Bt];
-      std::vector<double> qcols(cols.size());
-      for (size_t c = 0; c < cols.size(); ++c) qcols[c] = Q[cols[c]];
-      std::vector<long long> cum_np(cols.size() + 1, 0);
-      for (size_t c = 0; c < cols.size(); ++c) cum_np[c + 1] = cum_np[c] + o->pair_nprim[cols[c]];
-      // FP32 recurrences only where they replace real work (total l >= 4) and where the estimated
-      // FP32 error of the quartet, kFp32ErrScale * (qp amp)_ab * (qp amp)_cd * c2s amplification,
-      // stays below fp32_budget.  qp is the primitive-absolute bound sum_ab q_ab; amp bounds the
-      // cancellation of the recurrences (checked against an FP32 emulation of the recurrences on
-      // random quartets of mixed-exponent molecules: the error stayed below 12 * 2^-24 * bound * amp).
-      const bool fp32_class = fp32_budget > 0 && t.li + t.lj + t.lk + t.ll >= 4;
-      const double fp32_thr =
-          fp32_budget / (kFp32ErrScale * c2s_amp(t.li, p->sph) * c2s_amp(t.lj, p->sph) * c2s_amp(t.lk, p->sph) *
-                         c2s_amp(t.ll, p->sph));
-      // suffix maxima of qp*amp over the Q-sorted columns: the FP32 tail of a row starts where
-      // (qp amp)_row * (largest qp amp still ahead) < fp32_thr
-      std::vector<double> qp_sufmax(cols.size() + 1, 0.0);
-      if (fp32_class)
-        for (size_t c = cols.size(); c-- > 0;)
-          qp_sufmax[c] = std::max(qp_sufmax[c + 1], o->pair_qp[cols[c]] * o->pair_amp[cols[c]]);
-      // each row's partner prefix [0, cnt) splits into FP64 columns [0, c64) and FP32 columns
-      // [c64, cnt)
-      Tile t32 = t;
-      t32.fp32 = true;
-      t.row_prefix.push_back(0);
-      t32.row_prefix.push_back(0);
-      for (size_t r = 0; r < rows.size(); ++r) {
-        const double qa = Q[rows[r]];
-        // count of cols with qa * Q >= cutoff (cols sorted decreasing)
-        long long cnt = std::partition_point(qcols.begin(), qcols.end(), [&](double qb) { return qa * qb >= cutoff; }) -
-                        qcols.begin();
-        if (A == Bt) cnt = std::min<long long>(cnt, (long long)r + 1);
-        if (cnt <= 0) continue;
-        long long c64 = cnt;
-        if (fp32_class) {
-          const double qpa = o->pair_qp[rows[r]] * o->pair_amp[rows[r]];
-          c64 = std::partition_point(qp_sufmax.begin(), qp_sufmax.begin() + cols.size(),
-                                     [&](double m) { return qpa * m >= fp32_thr; }) - qp_sufmax.begin();
-          c64 = std::min(c64, cnt);
-        }
-        if (c64 > 0) {
-          t.rows.push_back(rows[r]);
-          t.row_prefix.push_back(t.row_prefix.back() + c64);
-        }
-        if (cnt > c64) {
-          t32.rows.push_back(rows[r]);
-          t32.colstart.push_back((int)c64);
-          t32.row_prefix.push_back(t32.row_prefix.back() + (cnt - c64));
-        }
+  // tiles A >= B in type order (types are ordered by (la, lb, ...), so classes are valid); one
+  // task per (A, B), run on host threads (each task owns its result), joined in (A, B) order
+  struct TileJob {
+    std::vector<Tile> tiles;
+    long long nq = 0, nint = 0, nq32 = 0;
+  };
+  auto make_tiles = [&](int A, int Bt, TileJob& R) {
+    Tile t;
+    t.typeA = A;
+    t.typeB = Bt;
+    t.li = std::get<0>(tkeys[A]);
+    t.lj = std::get<1>(tkeys[A]);
+    t.lk = std::get<0>(tkeys[Bt]);
+    t.ll = std::get<1>(tkeys[Bt]);
+    t.st = canonical_strides(t.li, t.lj, t.lk, p->sph);
+    // equal-l pairs are reported (other, centre): their two axes trade strides
+    if (t.li == t.lj) std::swap(t.st.s0, t.st.s1);
+    if (t.lk == t.ll) std::swap(t.st.s2, t.st.s3);
+    const std::vector<int>& rows = tlist[A];
+    const std::vector<int>& cols = tlist[Bt];
+    std::vector<double> qcols(cols.size());
+    for (size_t c = 0; c < cols.size(); ++c) qcols[c] = Q[cols[c]];
+    std::vector<long long> cum_np(cols.size() + 1, 0);
+    for (size_t c = 0; c < cols.size(); ++c) cum_np[c + 1] = cum_np[c] + o->pair_nprim[cols[c]];
+    // FP32 recurrences only where they replace real work (total l >= 4) and where the estimated
+    // FP32 error of the quartet, kFp32ErrScale * (qp amp)_ab * (qp amp)_cd * c2s amplification,
+    // stays below fp32_budget.  qp is the primitive-absolute bound sum_ab q_ab; amp bounds the
+    // cancellation of the recurrences (checked against an FP32 emulation of the recurrences on
+    // random quartets of mixed-exponent molecules: the error stayed below 12 * 2^-24 * bound * amp).
+    const bool fp32_class = fp32_budget > 0 && t.li + t.lj + t.lk + t.ll >= 4;
+    const double fp32_thr =
+        fp32_budget / (kFp32ErrScale * c2s_amp(t.li, p->sph) * c2s_amp(t.lj, p->sph) * c2s_amp(t.lk, p->sph) *
+                       c2s_amp(t.ll, p->sph));
+    // suffix maxima of qp*amp over the Q-sorted columns: the FP32 tail of a row starts where
+    // (qp amp)_row * (largest qp amp still ahead) < fp32_thr
+    std::vector<double> qp_sufmax(cols.size() + 1, 0.0);
+    if (fp32_class)
+      for (size_t c = cols.size(); c-- > 0;)
+        qp_sufmax[c] = std::max(qp_sufmax[c + 1], o->pair_qp[cols[c]] * o->pair_amp[cols[c]]);
+    // each row's partner prefix [0, cnt) splits into FP64 columns [0, c64) and FP32 columns
+    // [c64, cnt)
+    Tile t32 = t;
+    t32.fp32 = true;
+    t.row_prefix.push_back(0);
+    t32.row_prefix.push_back(0);
+    for (size_t r = 0; r < rows.size(); ++r) {
+      const double qa = Q[rows[r]];
+      // count of cols with qa * Q >= cutoff (cols sorted decreasing)
+      long long cnt = std::partition_point(qcols.begin(), qcols.end(), [&](double qb) { return qa * qb >= cutoff; }) -
+                      qcols.begin();
+      if (A == Bt) cnt = std::min<long long>(cnt, (long long)r + 1);
+      if (cnt <= 0) continue;
+      long long c64 = cnt;
+      if (fp32_class) {
+        const double qpa = o->pair_qp[rows[r]] * o->pair_amp[rows[r]];
+        c64 = std::partition_point(qp_sufmax.begin(), qp_sufmax.begin() + cols.size(),
+                                   [&](double m) { return qpa * m >= fp32_thr; }) - qp_sufmax.begin();
+        c64 = std::min(c64, cnt);
       }
-      const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
-                             nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
-      for (Tile* tp : {&t, &t32}) {
-        if (tp->rows.empty()) continue;
-        tp->cols = cols;
-        tp->cum_np = cum_np;
-        const long long nq = tp->row_prefix.back();
-        nq_total += nq;
-        nint_total += nq * nout;
-        if (tp->fp32) nq_fp32 += nq;
-        p->tiles.push_back(*tp);
+      if (c64 > 0) {
+        t.rows.push_back(rows[r]);
+        t.row_prefix.push_back(t.row_prefix.back() + c64);
+      }
+      if (cnt > c64) {
+        t32.rows.push_back(rows[r]);
+        t32.colstart.push_back((int)c64);
+        t32.row_prefix.push_back(t32.row_prefix.back() + (cnt - c64));
       }
     }
+    const long long nout = (long long)nsph_or_cart(t.li, p->sph) * nsph_or_cart(t.lj, p->sph) *
+                           nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
+    for (Tile* tp : {&t, &t32}) {
+      if (tp->rows.empty()) continue;
+      tp->cols = cols;
+      tp->cum_np = cum_np;
+      const long long nq = tp->row_prefix.back();
+      R.nq += nq;
+      R.nint += nq * nout;
+      if (tp->fp32) R.nq32 += nq;
+      R.tiles.push_back(std::move(*tp));
+    }
+  };
+  std::vector<std::pair<int, int>> jobs;
+  for (int A = 0; A < nt; ++A)
+    for (int Bt = 0; Bt <= A; ++Bt) jobs.emplace_back(A, Bt);
+  std::vector<TileJob> res(jobs.size());
+  {
+    std::atomic<size_t> next(0);
+    auto worker = [&]() {
+      for (size_t j; (j = next.fetch_add(1)) < jobs.size();) make_tiles(jobs[j].first, jobs[j].second, res[j]);
+    };
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int i = 1; i < std::min<int>(nthr, (int)jobs.size()); ++i) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
   }
-  return finish_screened(p, o, ecut, max_chunk, prim_budget, nq_total, nint_total, nq_fp32, plan);
+  for (TileJob& R : res) {
+    nq_total += R.nq;
+    nint_total += R.nint;
+    nq_fp32 += R.nq32;
+    for (Tile& t : R.tiles) p->tiles.push_back(std::move(t));
+  }
+  plog.mark("tiles (host)");
+  const int rcf = finish_screened(p, o, ecut, max_chunk, prim_budget, nq_total, nint_total, nq_fp32, plan);
+  plog.mark("chunks, segments, device tables");
+  return rcf;
 }
 
 // Diagonal Schwarz factors sqrt(max |block|) of a list of tuples of one family (spherical).
