@@ -29,14 +29,26 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
 
 static_assert(kNumVariants == kLaunchVariants, "variant count differs between kernel and host headers");
 
+// a split-transfer variant (10, 11) that is not compiled for the class runs the default shape
+static bool splitcoop_applies(int li, int lj, int lk, int ll, int variant) {
+  return variant_splitcoop(variant) && li <= CINTX_LMAX && splitcoop_dims(li, lj, lk, ll, splitcoop_acc(variant)).ok;
+}
+
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  if (variant_splitcoop(variant))
+    return splitcoop_applies(li, lj, lk, ll, variant) ? pick_threads(li, lj, lk, ll, splitcoop_acc(variant))
+                                                      : pick_threads(li, lj, lk, ll, variant_acc(0));
   if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   return pick_threads(li, lj, lk, ll, variant_acc(variant)) / variant_passes(variant);
 }
 
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
+  if (variant_splitcoop(variant)) {
+    if (!splitcoop_applies(li, lj, lk, ll, variant)) variant = 0;
+    else return (1 << 23) + pick_threads(li, lj, lk, ll, splitcoop_acc(variant)) * 1024 + kSplitCoopRegs;
+  }
   if (variant_sliced(variant) && !sliced_ok(li, lj, lk, ll, variant)) variant = 0;
   const int s = pick_threads(li, lj, lk, ll, variant_acc(variant));
   if (s == 1) return 1;  // one-lane shapes take no register cap

@@ -68,8 +68,9 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // hand-offs); the lanes meet only for the cartesian-to-spherical stages.
 // Variants 7 and 8 are variants 5 and 4 with the root loop rolled (a quarter to a fifth of the
 // code per slice: the slices' bodies compete for the instruction cache).  Variant 9 runs the eight
-// slices of variant 6 on four warps, two slices after one another per warp.
-constexpr int kNumVariants = 10;
+// slices of variant 6 on four warps, two slices after one another per warp.  Variants 10 and 11
+// are cooperative shapes with the horizontal transfers split over all lanes (eri_splitcoop.cuh).
+constexpr int kNumVariants = 12;
 __host__ __device__ constexpr int variant_acc(int v) {
   return v == 1 || v == 5 || v == 6 || v == 7 || v == 9 ? 48 : (v == 2 ? 12 : (v == 4 || v == 8 ? 32 : 24));
 }

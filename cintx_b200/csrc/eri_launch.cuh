@@ -37,6 +37,10 @@ __host__ __device__ constexpr bool class_valid(int li, int lj, int lk, int ll) {
 
 int device_sm_count();
 
+}  // namespace cintx
+#include "eri_splitcoop.cuh"
+namespace cintx {
+
 template <int LI, int LJ, int LK, int LL, bool SPH, class R = double, int ACC = 24, int REGS = 128,
           bool SLICE = false, bool ROLL = false, int PASSES = 1>
 cudaError_t launch_eri(const LaunchArgs& a) {
@@ -151,6 +155,18 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
             if (!done && a.variant == 9) {
               err = launch_eri<LI, LJ, k, l, true, double, variant_acc(9), variant_regs(9), true, true,
                                variant_passes(9)>(a);
+              done = true;
+            }
+          }
+          if constexpr (splitcoop_dims(LI, LJ, k, l, splitcoop_acc(10)).ok) {
+            if (!done && a.variant == 10) {
+              err = launch_splitcoop<LI, LJ, k, l, splitcoop_acc(10)>(a);
+              done = true;
+            }
+          }
+          if constexpr (splitcoop_dims(LI, LJ, k, l, splitcoop_acc(11)).ok) {
+            if (!done && a.variant == 11) {
+              err = launch_splitcoop<LI, LJ, k, l, splitcoop_acc(11)>(a);
               done = true;
             }
           }

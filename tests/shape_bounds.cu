@@ -1,11 +1,12 @@
 // Host-only enumeration of every launch shape the ERI dispatch compiles (test infrastructure).
 //
 // For each valid class (li lj | lk ll) and each shape dispatch_lij instantiates (spherical FP64
-// variants 0..9 where they apply, cartesian FP64, spherical FP32), prints one line
+// variants 0..11 where they apply, cartesian FP64, spherical FP32), prints one line
 //   li lj lk ll kind variant S LANES BLOCK Q B_GROUP SMEM_BYTES GLOBAL_BUF violation
-// where violation is shape_violation<Shape>() (0: every shared-memory, scratch, barrier and
-// per-thread index the kernel forms from the shape stays inside its buffer).  Compiled with nvcc
-// as a host program; it launches nothing.
+// where violation is shape_violation<Shape>() for eri4c_kernel's shapes and splitcoop_violation
+// for the split-transfer cooperative shapes (variants 10, 11) (0: every shared-memory, scratch,
+// barrier and per-thread index the kernel forms from the shape stays inside its buffer).
+// Compiled with nvcc as a host program; it launches nothing.
 #include <cstdio>
 
 #include "../cintx_b200/csrc/eri_launch.cuh"
@@ -41,6 +42,14 @@ void shapes_of_class() {
   if constexpr (sliced_ok(LI, LJ, LK, LL, 9))
     row<EriShape<LI, LJ, LK, LL, true, double, variant_acc(9), variant_regs(9), true, true, variant_passes(9)>>(
         LI, LJ, LK, LL, "sph", 9);
+  static_for<2>([&](auto V) {
+    constexpr int v = 10 + decltype(V)::value;
+    constexpr int acc = splitcoop_acc(v);
+    constexpr SplitCoopDims d = splitcoop_dims(LI, LJ, LK, LL, acc);
+    if constexpr (d.ok)
+      std::printf("%d %d %d %d %s %d %d %d %d %d %d %d %d %d\n", LI, LJ, LK, LL, "sph", v, d.S, d.S, d.BLOCK, d.Q,
+                  d.B_GROUP, d.SMEM_BYTES, 0, splitcoop_violation<LI, LJ, LK, LL, acc>());
+  });
 }
 
 int main() {

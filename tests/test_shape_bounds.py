@@ -31,5 +31,7 @@ def test_every_compiled_launch_shape_keeps_its_indexes_in_bounds(tmp_path):
         assert block <= 1024 and smem <= 227 * 1024
         if glob:  # classes whose transform buffers live in global scratch: one group per block
             assert q == 1
-    # the sliced shapes exist where the autotuner can pick them
+    # the sliced and split-transfer cooperative shapes exist where the autotuner can pick them
     assert any(r[4] == "sph" and r[5] == "9" for r in rows)
+    for v in ("10", "11"):
+        assert any(r[4] == "sph" and r[5] == v and r[:4] == ["3", "3", "3", "0"] for r in rows)
