@@ -684,6 +684,61 @@ def roofline_record(per_class, peak64, st, ms_per_step):
             "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
 
 
+def per_call_latency(cx, reps=3):
+    """The drop-in per-call path (int2e_sph with libcint's signature: one block per call, host in
+    and out, one device round trip) against libcint's own int2e_sph on the same calls (CPU, one
+    thread): every 8-fold-unique quartet of the 3-atom water-like molecule, called one after
+    another through ctypes with prepared arguments, with and without an optimizer.  The ctypes
+    cost of one call (a call of an empty library function) is reported beside them."""
+    import ctypes
+
+    from oracle import RefLibcint
+    mol = M.water_like()
+    nb = mol.nbas
+    quart = [(i, j, k, l) for i in range(nb) for j in range(i + 1) for k in range(i + 1) for l in range(k + 1)
+             if (i * (i + 1) // 2 + j) >= (k * (k + 1) // 2 + l)]
+    shls = np.ascontiguousarray(quart, dtype=np.int32)
+    atm, bas, env = (np.ascontiguousarray(a) for a in (mol.atm, mol.bas, mol.env))
+    out = np.zeros(4096)
+    P = ctypes.POINTER
+    ip = lambda a: a.ctypes.data_as(P(ctypes.c_int))
+    dp = lambda a: a.ctypes.data_as(P(ctypes.c_double))
+    args = (ip(atm), atm.shape[0], ip(bas), bas.shape[0], dp(env))
+    rows = [ip(shls[q]) for q in range(len(shls))]
+
+    def run(f, opt):
+        po = dp(out)
+        best = 1e300
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            for r in rows:
+                f(po, None, r, *args, opt, None)
+            best = min(best, time.perf_counter() - t0)
+        return 1e6 * best / len(rows)
+
+    ours = cx.lib.int2e_sph
+    ref = RefLibcint()
+    lcint = ref.lib.int2e_sph
+    o = cx.Optimizer(mol.atm, mol.bas, mol.env)
+    lopt = ctypes.c_void_p()
+    ref.lib.int2e_optimizer(ctypes.byref(lopt), *args)
+    run(ours, None)  # warm-up: device state, thread scratch
+    rec = {"quartets": len(rows), "molecule": "water-like, 3 atoms, %d shells" % nb,
+           "us_per_call_ours": run(ours, None), "us_per_call_ours_opt": run(ours, o.handle),
+           "us_per_call_libcint": run(lcint, None), "us_per_call_libcint_opt": run(lcint, lopt)}
+    noop = cx.lib.cintx_cuda_last_error_code
+    t0 = time.perf_counter()
+    for _ in rows:
+        noop()
+    rec["us_ctypes_call"] = 1e6 * (time.perf_counter() - t0) / len(rows)
+    ref.lib.CINTdel_optimizer(ctypes.byref(lopt))
+    o.close()
+    rec["what"] = ("libcint-signature int2e_sph per call (one block, host in/out: one H2D copy, one kernel, one D2H "
+                   "copy and a stream synchronisation per call) vs libcint 6.1.3 int2e_sph on the host, same "
+                   "quartets, best of %d passes; both through ctypes with prepared arguments" % reps)
+    return rec
+
+
 def learned_root_sample(cx, torch, opt, plan, mol, stream, n, seed):
     """Learned Rys roots on a seeded uniform sample of the sweep's quartets (an explicit plan: its
     root buffer holds every primitive quartet's roots, which the full sweep's 1e10 primitive
@@ -814,6 +869,9 @@ def our_arm(args):
     jk = None
     if rank == 0 and world == 1 and not args.no_jk:
         jk = jk_timing(cx, torch, plan, mol, stream, min(args.steps, 5))
+    per_call = None
+    if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
+        per_call = per_call_latency(cx)
 
     # end-to-end through the C ABI from host arrays, measured on every rank over its own chunks:
     # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory;
@@ -948,6 +1006,8 @@ def our_arm(args):
         line["error_vs_libcint"] = err_lib
     if jk is not None:
         line["jk_build"] = jk
+    if per_call is not None:
+        line["per_call"] = per_call
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
@@ -1026,35 +1086,54 @@ def df_arm(args):
     e2e = None
     if not args.no_e2e:
         # end to end from host arrays on every rank: optimizer, both plans, evaluation of the rank's
-        # 3-centre chunks (rank 0 also the 2-centre metric) and D2H of each into a page-locked host
-        # buffer (one chunk at a time: the 3-centre output exceeds host memory); max over ranks
-        host = torch.empty(max(s3.max_chunk_doubles, s2.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
-        times = []
-        for s_ in range(2):
+        # 3-centre chunks (rank 0 also the 2-centre metric) and D2H of each into page-locked host
+        # memory; at N = 1 the 3-centre sweep runs in chunks of --e2e-chunk-doubles through a
+        # two-slot host ring (copies overlap the next chunk's kernels), as the int2e e2e; max over ranks
+        e2e_chunk = args.e2e_chunk_doubles
+        ring = host2 = None
+        phases = {"optimizer": [], "plan": [], "execute_d2h": []}
+        for s_ in range(1 + max(1, min(args.steps, 3))):
             if world > 1:
                 dist.barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             o2 = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
-            e3, e2 = make(o2)
+            t1 = time.perf_counter()
+            e3 = cx.Plan.screened_3c(o2, norb, SCHWARZ, max_chunk_doubles=e2e_chunk)
+            e2 = cx.Plan.shells(o2, cx.INT2C2E, aux_pairs)
             if tuned and not args.no_autotune:
                 e3.use_tuned_shapes()
                 e2.use_tuned_shapes()
-            for c in chunks_of(assign_chunks([float(e3.segments(c)[2].sum()) for c in range(e3.stats.nchunks)],
-                                             world), rank):
-                e3.execute_host(host, chunk=c)
+            t2 = time.perf_counter()
+            if ring is None:  # page-locked host buffers, allocated in the untimed first iteration
+                ring = torch.empty(2 * max(e3.stats.max_chunk_doubles, 1), dtype=torch.float64,
+                                   pin_memory=True).numpy()
+                host2 = torch.empty(max(e2.stats.nintegrals, 1), dtype=torch.float64, pin_memory=True).numpy()
+            if world == 1:
+                e3.execute_host_ring(ring)
+            else:
+                for c in chunks_of(assign_chunks([float(e3.segments(c)[2].sum()) for c in range(e3.stats.nchunks)],
+                                                 world), rank):
+                    e3.execute_host(ring, chunk=c)
             if rank == 0:
-                e2.execute_host(host)
-            times.append(time.perf_counter() - t0)
+                e2.execute_host(host2)
+            t3 = time.perf_counter()
+            if s_ > 0:
+                phases["optimizer"].append(t1 - t0)
+                phases["plan"].append(t2 - t1)
+                phases["execute_d2h"].append(t3 - t2)
             h2d = mol.atm.nbytes + mol.bas.nbytes + mol.env.nbytes + o2.device_bytes + e3.stats.device_bytes
             e3.close()
             e2.close()
             o2.close()
-        te = max_over_ranks(times[-1], device="cuda")
+        te = max_over_ranks(sum(statistics.mean(v) for v in phases.values()), device="cuda")
         e2e = {"value": nint / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d) * world,
-               "d2h_bytes_per_step": int(nint * 8), "seconds_per_step": te, "ranks_timed": world,
+               "d2h_bytes_per_step": int(nint * 8), "seconds_per_step": te,
+               "phases_s": {k: statistics.mean(v) for k, v in phases.items()}, "chunk_doubles": e2e_chunk,
+               "ranks_timed": world,
                "includes": "optimizer from host atm/bas/env, both plans (Schwarz passes), evaluation and "
-                           "D2H of every integral, chunk by chunk, each rank its own chunks; max over ranks"}
+                           "D2H of every integral (each rank its own chunks; a two-chunk page-locked host ring "
+                           "overlapping copies with the next chunk's kernels at N=1); max over ranks"}
     if rank != 0:
         if world > 1:
             dist.barrier()

@@ -181,6 +181,8 @@ __global__ void __launch_bounds__(splitcoop_dims(LI, LJ, LK, LL, ACC).BLOCK, spl
   constexpr SplitCoopDims D = splitcoop_dims(LI, LJ, LK, LL, ACC);
   static_assert(D.ok && splitcoop_violation<LI, LJ, LK, LL, ACC>() == 0,
                 "an index of this launch shape can leave its buffer");
+  static_assert(D.B_GROUP % 16 == 0 && (SH::NI % 2 != 0 || (SH::GSZ % 2 == 0 && (2 * SH::NR) % 2 == 0)),
+                "16-byte loads of the I arrays need 16-byte aligned group regions and tables");
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr int NIJ = SH::NIJ, NKL = SH::NKL, NJ = SH::NJ, NL = SH::NL;
   extern __shared__ __align__(16) double smem[];
@@ -256,11 +258,17 @@ __global__ void __launch_bounds__(splitcoop_dims(LI, LJ, LK, LL, ACC).BLOCK, spl
           const double* gy = s_g + (1 * NR + r) * GSZ;
           const double* gz = s_g + (2 * NR + r) * GSZ;
 #pragma unroll
-          for (int k = 0; k < TPT; ++k)
-#pragma unroll
-            for (int fi = 0; fi < NFI; ++fi)
-              acc[k][fi] = fma(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
-                               gz[cart_z(LI, fi) + lt.oz[k]], acc[k][fi]);
+          for (int k = 0; k < TPT; ++k) {
+            double ix[SH::NI], iy[SH::NI], iz[SH::NI];
+            load_i_column<SH::NI>(ix, gx + lt.ox[k]);
+            load_i_column<SH::NI>(iy, gy + lt.oy[k]);
+            load_i_column<SH::NI>(iz, gz + lt.oz[k]);
+            static_loop(std::make_integer_sequence<int, NFI>{}, [&](auto c) {  // fi constant: ix, iy, iz stay in registers
+              constexpr int fi = decltype(c)::value;
+              constexpr int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
+              acc[k][fi] = fma(ix[cx] * iy[cy], iz[cz], acc[k][fi]);
+            });
+          }
         }
         group_sync<S>(group);
       }

@@ -120,6 +120,9 @@ struct CintxPlan {
   QuartetRec* d_recs = nullptr;    // explicit: all records; screened: one chunk's records
   long long rec_capacity = 0;
   char* d_tile_pool = nullptr;     // screened: every tile's rows, cols, prefix and colstart arrays
+  // work-queue counters of persistent-grid launches (variant 12): one per stream the plan launches on
+  int* d_queue = nullptr;
+  std::vector<cudaStream_t> queue_streams;
   std::vector<QuartetRec> h_recs;  // explicit plans keep a host copy for chunk_quartets
   std::vector<int> h_tuples;       // explicit: requested tuples (4 per record, -1 for unit)
   CintxPlanStats stats{};
@@ -155,6 +158,9 @@ void free_plan_device(CintxPlan* p) {
   p->d_recs = nullptr;
   if (p->d_tile_pool) cudaFree(p->d_tile_pool);  // the tiles' arrays live in it
   p->d_tile_pool = nullptr;
+  if (p->d_queue) cudaFree(p->d_queue);
+  p->d_queue = nullptr;
+  p->queue_streams.clear();
   for (Tile& t : p->tiles) {
     t.d_colstart = nullptr;
     t.d_rows = t.d_cols = nullptr;
@@ -394,6 +400,22 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   return CINTX_STATUS_SUCCESS;
 }
 
+constexpr int kQueueSlots = 64;
+
+// The plan's work-queue counter for launches on `stream` (allocated on first use; a plan about to
+// be captured into a graph allocates it before the capture starts), or nullptr.
+static int* queue_slot(CintxPlan* p, cudaStream_t stream) {
+  if (!p->d_queue && cudaMalloc(&p->d_queue, sizeof(int) * kQueueSlots) != cudaSuccess) {
+    p->d_queue = nullptr;
+    return nullptr;
+  }
+  for (size_t i = 0; i < p->queue_streams.size(); ++i)
+    if (p->queue_streams[i] == stream) return p->d_queue + i;
+  if ((int)p->queue_streams.size() >= kQueueSlots) return nullptr;
+  p->queue_streams.push_back(stream);
+  return p->d_queue + (p->queue_streams.size() - 1);
+}
+
 static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStream_t stream, DeviceState* ds,
                        ThreadScratch* ts) {
   const Opt* o = p->opt;
@@ -425,13 +447,27 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
     recs = dst;
     nrec = sg.t1 - sg.t0;
   }
+  // persistent-grid launches take a work-queue counter, zeroed in stream order before each launch
+  int* queue = nullptr;
+  if (variant_uses_queue(sg.li, sg.lj, sg.lk, sg.ll, p->sph, sg.fp32, sg.variant)) {
+    queue = queue_slot(p, stream);
+    if (!queue) {
+      set_error(CINTX_STATUS_ALLOCATION_FAILED, "work-queue counter unavailable");
+      return CINTX_STATUS_ALLOCATION_FAILED;
+    }
+  }
   // the kernels take an int count; split very large segments
   for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
     const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
     const bool rb = p->d_rootbuf && sg.tile == -1;  // learned roots: explicit plans only
+    if (queue && cudaMemsetAsync(queue, 0, sizeof(int), stream) != cudaSuccess) {
+      set_error(CINTX_STATUS_EXECUTION_FAILED, "work-queue reset failed");
+      return CINTX_STATUS_EXECUTION_FAILED;
+    }
     cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
                                  out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps,
-                                 sg.variant, rb ? p->d_rootbuf : nullptr, rb ? p->d_rootbase + sg.rec0 + r0 : nullptr);
+                                 sg.variant, rb ? p->d_rootbuf : nullptr, rb ? p->d_rootbase + sg.rec0 + r0 : nullptr,
+                                 queue);
     if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -1225,6 +1261,12 @@ int cintx_plan_graph_build(CintxPlan* p, const int64_t* chunks, int64_t n, doubl
     p->events.push_back(e);
   }
   cudaStream_t origin = p->branches[0];
+  // the work-queue counters are allocated here: no allocation may happen inside the capture
+  if (!p->d_queue && cudaMalloc(&p->d_queue, sizeof(int) * kQueueSlots) != cudaSuccess) {
+    p->d_queue = nullptr;
+    set_error(CINTX_STATUS_ALLOCATION_FAILED, "work-queue counters could not be allocated");
+    return CINTX_STATUS_ALLOCATION_FAILED;
+  }
   if (cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     set_error(CINTX_STATUS_EXECUTION_FAILED, "stream capture could not start");
     return CINTX_STATUS_EXECUTION_FAILED;
@@ -1486,8 +1528,9 @@ int compute_prim_schwarz(Opt* o) {
 // (la lb|la lb), batches of at most 2^25 doubles), block_absmax_sqrt_kernel reduces each block to
 // its factor, and only the factors come back to the host.  Same kernels, launch shapes and records
 // as an explicit plan of the tuples (a b a b), so the factors are those of that plan bit for bit.
-int diag_schwarz_2e(Opt* o, double ecut, std::vector<double>& Q) {
-  const int np = o->npairs;
+// np < 0: every stored pair; else the first np.
+int diag_schwarz_2e(Opt* o, double ecut, std::vector<double>& Q, int np) {
+  if (np < 0 || np > o->npairs) np = o->npairs;  // the first np stored pairs (all by default)
   Q.assign(np, 0.0);
   DeviceState* ds;
   ThreadScratch* ts;
@@ -1862,7 +1905,7 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
   const int np = o->npairs;
   // 1. Schwarz factors from the diagonal (ij|ij) blocks, spherical, reduced on the device
   std::vector<double> Q;
-  int rc = diag_schwarz_2e(o, expcutoff_2e(B.env.data()), Q);
+  int rc = diag_schwarz_2e(o, expcutoff_2e(B.env.data()), Q, -1);
   if (rc) return rc;
   plog.mark("diagonal Schwarz pass");
   // 2. pair types (la, lb, nprim_a, nprim_b), sorted pairs by decreasing Q
@@ -2050,17 +2093,15 @@ int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, 
   if (max_chunk <= 0) max_chunk = 1LL << 28;
   const int npo = norb * (norb + 1) / 2;  // pair ids of the orbital pairs (u < norb)
   const int naux = nb - norb;
-  // 1. Schwarz factors: (ab|ab) for orbital pairs, (k|k) for auxiliary shells
-  std::vector<int> dt((size_t)npo * 4), kt((size_t)naux * 2);
-  for (int id = 0; id < npo; ++id) {
-    dt[4 * id] = dt[4 * id + 2] = o->pair_a[id];
-    dt[4 * id + 1] = dt[4 * id + 3] = o->pair_b[id];
-  }
+  // 1. Schwarz factors: (ab|ab) for orbital pairs (reduced on the device), (k|k) for auxiliary shells
+  PhaseLog plog("int3c2e plan");
+  std::vector<int> kt((size_t)naux * 2);
   for (int k = 0; k < naux; ++k) kt[2 * k] = kt[2 * k + 1] = norb + k;
   std::vector<double> Q, Qk;
-  int rc = diag_factors(optp, CINTX_INT2E, dt, npo, Q);
+  int rc = diag_schwarz_2e(o, expcutoff_2e(B.env.data()), Q, npo);
   if (!rc) rc = diag_factors(optp, CINTX_INT2C2E, kt, naux, Qk);
   if (rc) return rc;
+  plog.mark("diagonal Schwarz passes");
   double qmax = 0, qkmax = 0;
   for (double v : Q) qmax = std::max(qmax, v);
   for (double v : Qk) qkmax = std::max(qkmax, v);
@@ -2128,7 +2169,10 @@ int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, 
       p->tiles.push_back(t);
     }
   }
-  return finish_screened(p, o, expcutoff_3c(B.env.data()), max_chunk, 0.0, nq_total, nint_total, 0, plan);
+  plog.mark("tiles (host)");
+  const int rcf = finish_screened(p, o, expcutoff_3c(B.env.data()), max_chunk, 0.0, nq_total, nint_total, 0, plan);
+  plog.mark("chunks, segments, device tables");
+  return rcf;
 }
 
 int64_t cintx_opt_device_bytes(CINTOpt* optp) {
