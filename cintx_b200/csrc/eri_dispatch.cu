@@ -7,8 +7,7 @@ namespace cintx {
 cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const QuartetRec* recs, int nrec,
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32,
-                         double prim_eps, int variant, const double* rootbuf, const long long* rootbase,
-                         int* queue) {
+                         double prim_eps, int variant, const double* rootbuf, const long long* rootbase) {
   LaunchArgs a;
   a.recs = recs;
   a.nrec = nrec;
@@ -25,7 +24,6 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
   a.variant = variant;
   a.rootbuf = rootbuf;
   a.rootbase = rootbase;
-  a.queue = queue;
   return dispatch_eri(li, lj, lk, ll, sph, a);
 }
 
@@ -34,12 +32,6 @@ static_assert(kNumVariants == kLaunchVariants, "variant count differs between ke
 // a split-transfer variant (10, 11) that is not compiled for the class runs the default shape
 static bool splitcoop_applies(int li, int lj, int lk, int ll, int variant) {
   return variant_splitcoop(variant) && li <= CINTX_LMAX && splitcoop_dims(li, lj, lk, ll, splitcoop_acc(variant)).ok;
-}
-
-// variant 12: the default shape of a one-lane class on a persistent grid fed by a device work queue
-bool variant_uses_queue(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
-  return variant == 12 && sph && !fp32 && li <= CINTX_LMAX && class_valid(li, lj, lk, ll) &&
-         pick_threads(li, lj, lk, ll, variant_acc(0)) == 1;
 }
 
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
@@ -52,7 +44,6 @@ int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int varia
 }
 
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant) {
-  if (variant_uses_queue(li, lj, lk, ll, sph, fp32, variant)) return (1 << 24) + 1;
   if (!sph || fp32 || variant <= 0 || variant >= kNumVariants) variant = 0;
   if (variant_splitcoop(variant)) {
     if (!splitcoop_applies(li, lj, lk, ll, variant)) variant = 0;

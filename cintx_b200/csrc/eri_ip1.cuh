@@ -154,16 +154,16 @@ __global__ void __launch_bounds__(Ip1Shape<LI, LJ, LK, LL, SPH>::BLOCK, 1)
               const int od = comp == 0 ? ox[k] : (comp == 1 ? oy[k] : oz[k]);
               const int oa = comp == 0 ? oy[k] : ox[k];
               const int ob = comp == 2 ? oy[k] : oz[k];
-#pragma unroll
-              for (int fi = 0; fi < NFI; ++fi) {
-                const int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
+              static_loop(std::make_integer_sequence<int, NFI>{}, [&](auto c) {  // fi a compile-time constant
+                constexpr int fi = decltype(c)::value;
+                constexpr int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
                 const int nd = comp == 0 ? cx : (comp == 1 ? cy : cz);
                 const int na = comp == 0 ? cy : cx;
                 const int nb = comp == 2 ? cy : cz;
                 double d = -ai2 * gd[nd + 1 + od];
                 if (nd > 0) d = fma((double)nd, gd[nd - 1 + od], d);
                 acc[k][fi] = fma(d * ga[na + oa], gb[nb + ob], acc[k][fi]);
-              }
+              });
             }
           }
           group_sync<S>(group);

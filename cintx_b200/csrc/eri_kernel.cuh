@@ -70,9 +70,7 @@ __host__ __device__ constexpr int pick_threads(int li, int lj, int lk, int ll, i
 // code per slice: the slices' bodies compete for the instruction cache).  Variant 9 runs the eight
 // slices of variant 6 on four warps, two slices after one another per warp.  Variants 10 and 11
 // are cooperative shapes with the horizontal transfers split over all lanes (eri_splitcoop.cuh).
-// Variant 12 runs a one-lane class's default shape on a persistent grid (one block per resident
-// slot) whose blocks take batches of quartets from a device work queue (LaunchArgs::queue).
-constexpr int kNumVariants = 13;
+constexpr int kNumVariants = 12;
 __host__ __device__ constexpr int variant_acc(int v) {
   return v == 1 || v == 5 || v == 6 || v == 7 || v == 9 ? 48 : (v == 2 ? 12 : (v == 4 || v == 8 ? 32 : 24));
 }
@@ -528,8 +526,7 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     eri4c_kernel(const QuartetRec* __restrict__ recs, int nrec, const ShellPair* __restrict__ pairs,
                  const PrimPair* __restrict__ prims, double* __restrict__ out, OutStrides st,
                  double expcutoff, const __grid_constant__ RysTable rys, double* __restrict__ gscratch,
-                 double prim_eps, const double* __restrict__ rootbuf, const long long* __restrict__ rootbase,
-                 int* __restrict__ queue) {
+                 double prim_eps, const double* __restrict__ rootbuf, const long long* __restrict__ rootbase) {
   using SH = EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SLICE, ROLL, PASSES>;
   constexpr int S = SH::S, NR = SH::NR, GSZ = SH::GSZ, NFI = SH::NFI, TPT = SH::TPT;
   constexpr bool FP64 = std::is_same<R, double>::value;
@@ -569,302 +566,274 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   // q = blockIdx.x * Q + group; in sliced shapes every thread of a set runs the trip count of the
   // set's first quartet (the set shares barriers) and lanes past the end only take part in them
   const int qfirst = SLICE ? (int)blockIdx.x * SH::Q + (group & ~31) : (int)blockIdx.x * SH::Q + group;
-  // Quartet loop.  Grid-stride by default; one-lane shapes given a work-queue counter (a
-  // persistent grid, one block per resident slot) take batches of Q quartets from it instead, all
-  // threads of a block together, until the queue runs past nrec.
-  int* s_batch = nullptr;  // one-lane shapes only (the others may fill all 227 KB of shared memory)
-  if constexpr (S == 1) {
-    __shared__ int batch;
-    s_batch = &batch;
-  }
-  const bool use_queue = S == 1 && queue != nullptr;
-  long long q0 = 0;  // the block's current batch (queue mode)
-  int qb = qfirst;
-  if (use_queue) {
-    if (threadIdx.x == 0) *s_batch = atomicAdd(queue, 1);
-    __syncthreads();
-    q0 = (long long)*s_batch * SH::Q;
-    qb = q0 + group < nrec ? (int)(q0 + group) : nrec;
-  }
-  while (use_queue ? q0 < nrec : qb < nrec) {
-    if (qb < nrec) {
-      const int qv = SLICE ? qb + (group & 31) : qb;
-      const bool live = !SLICE || qv < nrec;
-      const int q = live ? qv : nrec - 1;
-      const QuartetRec rec = recs[q];
-      // precomputed roots of this quartet's primitive quartets ([b][a][2*NR]), or table roots
-      const double* rb = rootbuf ? rootbuf + rootbase[q] : nullptr;
-      const ShellPair pij = pairs[rec.pij];
-      const ShellPair pkl = pairs[rec.pkl];
-      double acc[TPT][NFI];
-  #pragma unroll
-      for (int k = 0; k < TPT; ++k)
-  #pragma unroll
-        for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
+  for (int qb = qfirst; qb < nrec; qb += gridDim.x * SH::Q) {
+    const int qv = SLICE ? qb + (group & 31) : qb;
+    const bool live = !SLICE || qv < nrec;
+    const int q = live ? qv : nrec - 1;
+    const QuartetRec rec = recs[q];
+    // precomputed roots of this quartet's primitive quartets ([b][a][2*NR]), or table roots
+    const double* rb = rootbuf ? rootbuf + rootbase[q] : nullptr;
+    const ShellPair pij = pairs[rec.pij];
+    const ShellPair pkl = pairs[rec.pkl];
+    double acc[TPT][NFI];
+#pragma unroll
+    for (int k = 0; k < TPT; ++k)
+#pragma unroll
+      for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
 
-      if constexpr (S == 1) {
-        prim_loop_one_lane<LI, LJ, LK, LL, SH, R>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff,
-                                                  prim_eps, rb, lt, acc);
-      } else if constexpr (SLICE) {
-        // each lane runs the register path for its own tuple slice (lane + S*k)
-        static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
-          constexpr int sl = decltype(j)::value;
-          if (live && lane == sl % LN) {
-            prim_loop_one_lane<LI, LJ, LK, LL, SH, R, sl>(pij, pkl, prims, rys, nullptr, expcutoff, prim_eps, rb, lt,
-                                                          acc);
-            if constexpr (PASSES > 1) {
-              // stage i of this slice now: the next pass reuses the accumulators
-  #pragma unroll
-              for (int k = 0; k < TPT; ++k) {
-                const int t = sl + S * k;
-                if (t < SH::NTUP) {
-  #pragma unroll
-                  for (int mi = 0; mi < SH::MI; ++mi) {
-                    double v = 0.0;
-  #pragma unroll
-                    for (int fi = 0; fi < NFI; ++fi) {
-                      const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
-                      if (c != 0.0) v += c * acc[k][fi];
-                    }
-                    sg[mi + SH::MI * t] = v;
-                  }
-                }
-  #pragma unroll
-                for (int fi = 0; fi < NFI; ++fi) acc[k][fi] = 0.0;
-              }
-            }
-          }
-        });
-      } else
-      for (int b = 0; b < pkl.nprim; ++b) {
-        const PrimPair pk = prims[pkl.prim_off + b];
-        const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
-        const double qthr = prim_eps / pk.q;  // as in prim_loop_one_lane
-        for (int a = 0; a < pij.nprim; ++a) {
-          const PrimPair pi = prims[pij.prim_off + a];
-          if (pi.q < qthr) break;
-          if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
-          const double aij = pi.aij, akl = pk.aij;
-          const double aijkl = aij + akl;
-          const double rs = rsqrt(aijkl);
-          const double inv_aijkl = rs * rs;
-          const double a1 = aij * akl;
-          const double inv_a1 = 4.0 * pi.half_inv * pk.half_inv;
-          const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
-          const double rr = pqx * pqx + pqy * pqy + pqz * pqz;
-          const double x = a1 * inv_aijkl * rr;
-          const double fac = pi.kab * pk.kab * rs * inv_a1;
-          const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
-
-          // roots: the group's lanes split the 2*NR table polynomials (or copy precomputed ones)
-          if (rb) {
-            const double* r = rb + (size_t)(b * pij.nprim + a) * (2 * NR);
-            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = r[f];
-          } else if constexpr (SH::STAGE_TABLE) {
-            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
-          } else {
-            for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
-          }
-          group_sync<S>(group);
-          // (axis, root) recurrences, one per lane; coefficients in FP64, recurrences in R
-          for (int tp = lane; tp < 3 * NR * SH::NPARTS; tp += S) {
-            const int task = tp / SH::NPARTS, part = tp % SH::NPARTS;
-            const int axis = task / NR, r = task % NR;
-            const double t2 = s_roots[r];
-            const double rt_aa = t2 * inv_aijkl;
-            const double b00 = 0.5 * rt_aa;
-            const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
-            const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
-            const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
-            const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
-            const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
-            const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
-            const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
-            const double g00 = axis == 2 ? s_roots[NR + r] * fac : 1.0;
-            if constexpr (SH::REG_RECUR) {
-              vrr_hrr<LI, LJ, LK, LL, R>(s_g + task * GSZ, (R)g00, (R)(pa - rt_aa * akl * pq),
-                                         (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab, (R)cd);
-            } else {
-              vrr_hrr_smem<LI, LJ, LK, LL, R, SH::NPARTS>(s_g + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL),
-                                                          (R)g00, (R)(pa - rt_aa * akl * pq),
-                                                          (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab,
-                                                          (R)cd, part);
-            }
-          }
-          group_sync<S>(group);
-          // cartesian products, summed over roots (R), added to the FP64 accumulators
-          R part[FP64 ? 1 : TPT][FP64 ? 1 : NFI];
-          if constexpr (!FP64) {
-  #pragma unroll
-            for (int k2 = 0; k2 < TPT; ++k2)
-  #pragma unroll
-              for (int f2 = 0; f2 < NFI; ++f2) part[k2][f2] = (R)0;
-          }
-  #pragma unroll 1
-          for (int r = 0; r < NR; ++r) {
-            const R* gx = s_g + (0 * NR + r) * GSZ;
-            const R* gy = s_g + (1 * NR + r) * GSZ;
-            const R* gz = s_g + (2 * NR + r) * GSZ;
-  #pragma unroll
+    if constexpr (S == 1) {
+      prim_loop_one_lane<LI, LJ, LK, LL, SH, R>(pij, pkl, prims, rys, SH::STAGE_TABLE ? smem : nullptr, expcutoff,
+                                                prim_eps, rb, lt, acc);
+    } else if constexpr (SLICE) {
+      // each lane runs the register path for its own tuple slice (lane + S*k)
+      static_loop(std::make_integer_sequence<int, S>{}, [&](auto j) {
+        constexpr int sl = decltype(j)::value;
+        if (live && lane == sl % LN) {
+          prim_loop_one_lane<LI, LJ, LK, LL, SH, R, sl>(pij, pkl, prims, rys, nullptr, expcutoff, prim_eps, rb, lt,
+                                                        acc);
+          if constexpr (PASSES > 1) {
+            // stage i of this slice now: the next pass reuses the accumulators
+#pragma unroll
             for (int k = 0; k < TPT; ++k) {
-              if constexpr (FP64) {
-                double ix[SH::NI], iy[SH::NI], iz[SH::NI];
-                load_i_column<SH::NI>(ix, gx + lt.ox[k]);
-                load_i_column<SH::NI>(iy, gy + lt.oy[k]);
-                load_i_column<SH::NI>(iz, gz + lt.oz[k]);
-                static_loop(std::make_integer_sequence<int, NFI>{}, [&](auto c) {  // fi constant: ix, iy, iz stay in registers
-                  constexpr int fi = decltype(c)::value;
-                  constexpr int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
-                  acc[k][fi] = fma(ix[cx] * iy[cy], iz[cz], acc[k][fi]);
-                });
-              } else {
-  #pragma unroll
-                for (int fi = 0; fi < NFI; ++fi)
-                  part[k][fi] = fmaf(gx[cart_x(LI, fi) + lt.ox[k]] * gy[cart_y(LI, fi) + lt.oy[k]],
-                                     gz[cart_z(LI, fi) + lt.oz[k]], part[k][fi]);
+              const int t = sl + S * k;
+              if (t < SH::NTUP) {
+#pragma unroll
+                for (int mi = 0; mi < SH::MI; ++mi) {
+                  double v = 0.0;
+#pragma unroll
+                  for (int fi = 0; fi < NFI; ++fi) {
+                    const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+                    if (c != 0.0) v += c * acc[k][fi];
+                  }
+                  sg[mi + SH::MI * t] = v;
+                }
               }
+#pragma unroll
+              for (int fi = 0; fi < NFI; ++fi) acc[k][fi] = 0.0;
             }
           }
-          if constexpr (!FP64) {
-  #pragma unroll
-            for (int k2 = 0; k2 < TPT; ++k2)
-  #pragma unroll
-              for (int f2 = 0; f2 < NFI; ++f2) acc[k2][f2] += (double)part[k2][f2];
-          }
-          group_sync<S>(group);
         }
-      }
+      });
+    } else
+    for (int b = 0; b < pkl.nprim; ++b) {
+      const PrimPair pk = prims[pkl.prim_off + b];
+      const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
+      const double qthr = prim_eps / pk.q;  // as in prim_loop_one_lane
+      for (int a = 0; a < pij.nprim; ++a) {
+        const PrimPair pi = prims[pij.prim_off + a];
+        if (pi.q < qthr) break;
+        if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
+        const double aij = pi.aij, akl = pk.aij;
+        const double aijkl = aij + akl;
+        const double rs = rsqrt(aijkl);
+        const double inv_aijkl = rs * rs;
+        const double a1 = aij * akl;
+        const double inv_a1 = 4.0 * pi.half_inv * pk.half_inv;
+        const double pqx = pi.px - pk.px, pqy = pi.py - pk.py, pqz = pi.pz - pk.pz;
+        const double rr = pqx * pqx + pqy * pqy + pqz * pqz;
+        const double x = a1 * inv_aijkl * rr;
+        const double fac = pi.kab * pk.kab * rs * inv_a1;
+        const double pax = pi.px - pij.ax, pay = pi.py - pij.ay, paz = pi.pz - pij.az;
 
-      // ---- transform to spherical and store ----
-      double* const obase = out + rec.out;
-      if constexpr (S == 1) {
-        // whole block in registers: TPT == NTUP
-  #pragma unroll
-        for (int ml = 0; ml < SH::ML; ++ml)
-  #pragma unroll
-          for (int mk = 0; mk < SH::MK; ++mk)
-  #pragma unroll
-            for (int mj = 0; mj < SH::MJ; ++mj)
-  #pragma unroll
-              for (int mi = 0; mi < SH::MI; ++mi) {
-                double v = 0.0;
-  #pragma unroll
-                for (int fl = 0; fl < SH::NFL; ++fl) {
-                  constexpr bool sl = SPH && LL >= 2;
-                  const double cl = sl ? c2s_coef(LL, ml, fl) : (ml == fl ? 1.0 : 0.0);
-                  if (cl == 0.0) continue;
-  #pragma unroll
-                  for (int fk = 0; fk < SH::NFK; ++fk) {
-                    constexpr bool sk = SPH && LK >= 2;
-                    const double ck = sk ? c2s_coef(LK, mk, fk) : (mk == fk ? 1.0 : 0.0);
-                    if (ck == 0.0) continue;
-  #pragma unroll
-                    for (int fj = 0; fj < SH::NFJ; ++fj) {
-                      constexpr bool sj = SPH && LJ >= 2;
-                      const double cj = sj ? c2s_coef(LJ, mj, fj) : (mj == fj ? 1.0 : 0.0);
-                      if (cj == 0.0) continue;
-  #pragma unroll
-                      for (int fi = 0; fi < NFI; ++fi) {
-                        constexpr bool si = SPH && LI >= 2;
-                        const double ci = si ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
-                        if (ci == 0.0) continue;
-                        v += ci * cj * ck * cl * acc[fj + SH::NFJ * (fk + SH::NFK * fl)][fi];
-                      }
-                    }
-                  }
-                }
-                obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
-              }
-      } else {
-        double* bufA = SH::GLOBAL_BUF ? gscratch + (size_t)blockIdx.x * SH::GBUF_PER_BLOCK : sg;
-        double* bufB = bufA + SH::SM_BUFA;
-        // stage i in registers -> bufA[mi + MI * t], t = fj + NFJ*(fk + NFK*fl) (two-pass sliced
-        // shapes stored it after each pass)
-  #pragma unroll
-        for (int k = 0; k < TPT; ++k) {
-          const int t = lane + S * k;
-          if (PASSES == 1 && t < SH::NTUP) {
-  #pragma unroll
+        // roots: the group's lanes split the 2*NR table polynomials (or copy precomputed ones)
+        if (rb) {
+          const double* r = rb + (size_t)(b * pij.nprim + a) * (2 * NR);
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = r[f];
+        } else if constexpr (SH::STAGE_TABLE) {
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn_staged<NR>(smem, rys, f, x);
+        } else {
+          for (int f = lane; f < 2 * NR; f += S) s_roots[f] = rys_fn(rys, NR, f, x);
+        }
+        group_sync<S>(group);
+        // (axis, root) recurrences, one per lane; coefficients in FP64, recurrences in R
+        for (int tp = lane; tp < 3 * NR * SH::NPARTS; tp += S) {
+          const int task = tp / SH::NPARTS, part = tp % SH::NPARTS;
+          const int axis = task / NR, r = task % NR;
+          const double t2 = s_roots[r];
+          const double rt_aa = t2 * inv_aijkl;
+          const double b00 = 0.5 * rt_aa;
+          const double b10 = pi.half_inv * (1.0 - rt_aa * akl);
+          const double b01 = pk.half_inv * (1.0 - rt_aa * aij);
+          const double pa = axis == 0 ? pax : (axis == 1 ? pay : paz);
+          const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
+          const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
+          const double ab = axis == 0 ? pij.abx : (axis == 1 ? pij.aby : pij.abz);
+          const double cd = axis == 0 ? pkl.abx : (axis == 1 ? pkl.aby : pkl.abz);
+          const double g00 = axis == 2 ? s_roots[NR + r] * fac : 1.0;
+          if constexpr (SH::REG_RECUR) {
+            vrr_hrr<LI, LJ, LK, LL, R>(s_g + task * GSZ, (R)g00, (R)(pa - rt_aa * akl * pq),
+                                       (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab, (R)cd);
+          } else {
+            vrr_hrr_smem<LI, LJ, LK, LL, R, SH::NPARTS>(s_g + task * GSZ, s_scr + lane * (SH::NIJ * SH::NKL),
+                                                        (R)g00, (R)(pa - rt_aa * akl * pq),
+                                                        (R)(qc + rt_aa * aij * pq), (R)b10, (R)b01, (R)b00, (R)ab,
+                                                        (R)cd, part);
+          }
+        }
+        group_sync<S>(group);
+        // cartesian products, summed over roots (R), added to the FP64 accumulators
+        R part[FP64 ? 1 : TPT][FP64 ? 1 : NFI];
+        if constexpr (!FP64) {
+#pragma unroll
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) part[k2][f2] = (R)0;
+        }
+#pragma unroll 1
+        for (int r = 0; r < NR; ++r) {
+          const R* gx = s_g + (0 * NR + r) * GSZ;
+          const R* gy = s_g + (1 * NR + r) * GSZ;
+          const R* gz = s_g + (2 * NR + r) * GSZ;
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            if constexpr (FP64) {
+              double ix[SH::NI], iy[SH::NI], iz[SH::NI];
+              load_i_column<SH::NI>(ix, gx + lt.ox[k]);
+              load_i_column<SH::NI>(iy, gy + lt.oy[k]);
+              load_i_column<SH::NI>(iz, gz + lt.oz[k]);
+              static_loop(std::make_integer_sequence<int, NFI>{}, [&](auto c) {  // fi constant: ix, iy, iz stay in registers
+                constexpr int fi = decltype(c)::value;
+                constexpr int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
+                acc[k][fi] = fma(ix[cx] * iy[cy], iz[cz], acc[k][fi]);
+              });
+            } else {
+              static_loop(std::make_integer_sequence<int, NFI>{}, [&](auto c) {
+                constexpr int fi = decltype(c)::value;
+                constexpr int cx = cart_x(LI, fi), cy = cart_y(LI, fi), cz = cart_z(LI, fi);
+                part[k][fi] = fmaf(gx[cx + lt.ox[k]] * gy[cy + lt.oy[k]], gz[cz + lt.oz[k]], part[k][fi]);
+              });
+            }
+          }
+        }
+        if constexpr (!FP64) {
+#pragma unroll
+          for (int k2 = 0; k2 < TPT; ++k2)
+#pragma unroll
+            for (int f2 = 0; f2 < NFI; ++f2) acc[k2][f2] += (double)part[k2][f2];
+        }
+        group_sync<S>(group);
+      }
+    }
+
+    // ---- transform to spherical and store ----
+    double* const obase = out + rec.out;
+    if constexpr (S == 1) {
+      // whole block in registers: TPT == NTUP
+#pragma unroll
+      for (int ml = 0; ml < SH::ML; ++ml)
+#pragma unroll
+        for (int mk = 0; mk < SH::MK; ++mk)
+#pragma unroll
+          for (int mj = 0; mj < SH::MJ; ++mj)
+#pragma unroll
             for (int mi = 0; mi < SH::MI; ++mi) {
               double v = 0.0;
-  #pragma unroll
-              for (int fi = 0; fi < NFI; ++fi) {
-                const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
-                if (c != 0.0) v += c * acc[k][fi];
+#pragma unroll
+              for (int fl = 0; fl < SH::NFL; ++fl) {
+                constexpr bool sl = SPH && LL >= 2;
+                const double cl = sl ? c2s_coef(LL, ml, fl) : (ml == fl ? 1.0 : 0.0);
+                if (cl == 0.0) continue;
+#pragma unroll
+                for (int fk = 0; fk < SH::NFK; ++fk) {
+                  constexpr bool sk = SPH && LK >= 2;
+                  const double ck = sk ? c2s_coef(LK, mk, fk) : (mk == fk ? 1.0 : 0.0);
+                  if (ck == 0.0) continue;
+#pragma unroll
+                  for (int fj = 0; fj < SH::NFJ; ++fj) {
+                    constexpr bool sj = SPH && LJ >= 2;
+                    const double cj = sj ? c2s_coef(LJ, mj, fj) : (mj == fj ? 1.0 : 0.0);
+                    if (cj == 0.0) continue;
+#pragma unroll
+                    for (int fi = 0; fi < NFI; ++fi) {
+                      constexpr bool si = SPH && LI >= 2;
+                      const double ci = si ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+                      if (ci == 0.0) continue;
+                      v += ci * cj * ck * cl * acc[fj + SH::NFJ * (fk + SH::NFK * fl)][fi];
+                    }
+                  }
+                }
               }
-              bufA[mi + SH::MI * t] = v;
+              obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
             }
-          }
-        }
-        quartet_sync<LN, SLICE, SH::BLOCK>(group);
-        // stage j: bufA[mi + MI*(fj + NFJ*(fk + NFK*fl))] -> bufB[mi + MI*(mj + MJ*(fk + NFK*fl))]
-        const double* cur = bufA;
-        if constexpr (SPH && LJ >= 2) {
-          constexpr int n = SH::MI * SH::MJ * SH::NFK * SH::NFL;
-          for (int o = lane; o < n; o += LN) {
-            const int mi = o % SH::MI;
-            const int mj = (o / SH::MI) % SH::MJ;
-            const int rest = o / (SH::MI * SH::MJ);
-            const C2SRow& row = C2S_ROWS[LJ][mj];
-            double v = 0.0;
-            for (int z = 0; z < row.nnz; ++z) v += row.c[z] * bufA[mi + SH::MI * (row.f[z] + SH::NFJ * rest)];
-            bufB[o] = v;
-          }
-          quartet_sync<LN, SLICE, SH::BLOCK>(group);
-          cur = bufB;
-        }
-        // stage k: cur[mi + MI*(mj + MJ*(fk + NFK*fl))] -> nxt[mi + MI*(mj + MJ*(mk + MK*fl))]
-        if constexpr (SPH && LK >= 2) {
-          double* nxt = (cur == bufA) ? bufB : bufA;
-          constexpr int n = SH::MI * SH::MJ * SH::MK * SH::NFL;
-          for (int o = lane; o < n; o += LN) {
-            const int mij = o % (SH::MI * SH::MJ);
-            const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
-            const int fl = o / (SH::MI * SH::MJ * SH::MK);
-            const C2SRow& row = C2S_ROWS[LK][mk];
-            double v = 0.0;
-            for (int z = 0; z < row.nnz; ++z)
-              v += row.c[z] * cur[mij + SH::MI * SH::MJ * (row.f[z] + SH::NFK * fl)];
-            nxt[o] = v;
-          }
-          quartet_sync<LN, SLICE, SH::BLOCK>(group);
-          cur = nxt;
-        }
-        // stage l + store: cur[mijk + MIJK*fl] -> out
-        {
-          constexpr int n = SH::NOUT;
-          constexpr int MIJK = SH::MI * SH::MJ * SH::MK;
-          for (int o = lane; o < n; o += LN) {
-            const int mi = o % SH::MI;
-            const int mj = (o / SH::MI) % SH::MJ;
-            const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
-            const int ml = o / MIJK;
-            const int mijk = o % MIJK;
-            double v;
-            if constexpr (SPH && LL >= 2) {
-              const C2SRow& row = C2S_ROWS[LL][ml];
-              v = 0.0;
-              for (int z = 0; z < row.nnz; ++z) v += row.c[z] * cur[mijk + MIJK * row.f[z]];
-            } else {
-              v = cur[mijk + MIJK * ml];
-            }
-            if (live) obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
-          }
-        }
-        quartet_sync<LN, SLICE, SH::BLOCK>(group);
-      }
-      }
-    if (use_queue) {
-      __syncthreads();  // every thread has read the batch before thread 0 takes the next one
-      if (threadIdx.x == 0) *s_batch = atomicAdd(queue, 1);
-      __syncthreads();
-      q0 = (long long)*s_batch * SH::Q;
-      qb = q0 + group < nrec ? (int)(q0 + group) : nrec;
     } else {
-      qb += gridDim.x * SH::Q;
+      double* bufA = SH::GLOBAL_BUF ? gscratch + (size_t)blockIdx.x * SH::GBUF_PER_BLOCK : sg;
+      double* bufB = bufA + SH::SM_BUFA;
+      // stage i in registers -> bufA[mi + MI * t], t = fj + NFJ*(fk + NFK*fl) (two-pass sliced
+      // shapes stored it after each pass)
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) {
+        const int t = lane + S * k;
+        if (PASSES == 1 && t < SH::NTUP) {
+#pragma unroll
+          for (int mi = 0; mi < SH::MI; ++mi) {
+            double v = 0.0;
+#pragma unroll
+            for (int fi = 0; fi < NFI; ++fi) {
+              const double c = (SPH && LI >= 2) ? c2s_coef(LI, mi, fi) : (mi == fi ? 1.0 : 0.0);
+              if (c != 0.0) v += c * acc[k][fi];
+            }
+            bufA[mi + SH::MI * t] = v;
+          }
+        }
+      }
+      quartet_sync<LN, SLICE, SH::BLOCK>(group);
+      // stage j: bufA[mi + MI*(fj + NFJ*(fk + NFK*fl))] -> bufB[mi + MI*(mj + MJ*(fk + NFK*fl))]
+      const double* cur = bufA;
+      if constexpr (SPH && LJ >= 2) {
+        constexpr int n = SH::MI * SH::MJ * SH::NFK * SH::NFL;
+        for (int o = lane; o < n; o += LN) {
+          const int mi = o % SH::MI;
+          const int mj = (o / SH::MI) % SH::MJ;
+          const int rest = o / (SH::MI * SH::MJ);
+          const C2SRow& row = C2S_ROWS[LJ][mj];
+          double v = 0.0;
+          for (int z = 0; z < row.nnz; ++z) v += row.c[z] * bufA[mi + SH::MI * (row.f[z] + SH::NFJ * rest)];
+          bufB[o] = v;
+        }
+        quartet_sync<LN, SLICE, SH::BLOCK>(group);
+        cur = bufB;
+      }
+      // stage k: cur[mi + MI*(mj + MJ*(fk + NFK*fl))] -> nxt[mi + MI*(mj + MJ*(mk + MK*fl))]
+      if constexpr (SPH && LK >= 2) {
+        double* nxt = (cur == bufA) ? bufB : bufA;
+        constexpr int n = SH::MI * SH::MJ * SH::MK * SH::NFL;
+        for (int o = lane; o < n; o += LN) {
+          const int mij = o % (SH::MI * SH::MJ);
+          const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
+          const int fl = o / (SH::MI * SH::MJ * SH::MK);
+          const C2SRow& row = C2S_ROWS[LK][mk];
+          double v = 0.0;
+          for (int z = 0; z < row.nnz; ++z)
+            v += row.c[z] * cur[mij + SH::MI * SH::MJ * (row.f[z] + SH::NFK * fl)];
+          nxt[o] = v;
+        }
+        quartet_sync<LN, SLICE, SH::BLOCK>(group);
+        cur = nxt;
+      }
+      // stage l + store: cur[mijk + MIJK*fl] -> out
+      {
+        constexpr int n = SH::NOUT;
+        constexpr int MIJK = SH::MI * SH::MJ * SH::MK;
+        for (int o = lane; o < n; o += LN) {
+          const int mi = o % SH::MI;
+          const int mj = (o / SH::MI) % SH::MJ;
+          const int mk = (o / (SH::MI * SH::MJ)) % SH::MK;
+          const int ml = o / MIJK;
+          const int mijk = o % MIJK;
+          double v;
+          if constexpr (SPH && LL >= 2) {
+            const C2SRow& row = C2S_ROWS[LL][ml];
+            v = 0.0;
+            for (int z = 0; z < row.nnz; ++z) v += row.c[z] * cur[mijk + MIJK * row.f[z]];
+          } else {
+            v = cur[mijk + MIJK * ml];
+          }
+          if (live) obase[mi * st.s0 + mj * st.s1 + mk * st.s2 + ml * st.s3] = v;
+        }
+      }
+      quartet_sync<LN, SLICE, SH::BLOCK>(group);
     }
   }
-
 }
 
 }  // namespace cintx

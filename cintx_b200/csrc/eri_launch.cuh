@@ -23,8 +23,6 @@ struct LaunchArgs {
   int variant = 0;      // launch-shape variant (spherical FP64 classes; see variant_acc)
   const double* rootbuf = nullptr;     // precomputed roots [record's base + (b*npij + a)*2*NR]
   const long long* rootbase = nullptr;  // per record of this launch: its base in rootbuf
-  int* queue = nullptr;  // one-lane shapes: device work-queue counter (zeroed before the launch) for a
-                         // persistent grid, one block per resident slot; nullptr: grid-stride launch
 };
 
 // Device scratch for classes whose transform buffers live in global memory: returns a buffer
@@ -60,20 +58,6 @@ cudaError_t launch_eri(const LaunchArgs& a) {
   if (a.nrec <= 0) return cudaSuccess;
   long long blocks = ((long long)a.nrec + SH::Q - 1) / SH::Q;
   long long cap = a.max_blocks > 0 ? a.max_blocks : (long long)device_sm_count() * 32;
-  int* queue = nullptr;
-  if constexpr (SH::S == 1) {
-    if (a.queue) {  // persistent grid: as many blocks as fit on the device at once
-      static int resident[64];
-      if (dev < 64 && !resident[dev]) {
-        int nb = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, SH::BLOCK, SH::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        resident[dev] = nb > 0 ? nb : 1;
-      }
-      cap = (long long)device_sm_count() * (dev < 64 ? resident[dev] : 1);
-      queue = a.queue;
-    }
-  }
   if (blocks > cap) blocks = cap;
   double* scratch = nullptr;
   if constexpr (SH::GLOBAL_BUF) {
@@ -83,7 +67,7 @@ cudaError_t launch_eri(const LaunchArgs& a) {
   }
   kern<<<(unsigned)blocks, SH::BLOCK, SH::SMEM_BYTES, a.stream>>>(a.recs, a.nrec, a.pairs, a.prims, a.out,
                                                                    a.st, a.expcutoff, a.rys, scratch, a.prim_eps,
-                                                                   a.rootbuf, a.rootbase, queue);
+                                                                   a.rootbuf, a.rootbase);
   return cudaGetLastError();
 }
 
@@ -112,11 +96,11 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
           constexpr int s2 = pick_threads(LI, LJ, k, l, variant_acc(2));
           // only shapes that differ from the default are instantiated (if constexpr)
           bool done = false;
-          if (a.fp32 || !sph) {
-            LaunchArgs b = a;
-            b.queue = nullptr;  // the work queue: variant 12 of spherical FP64 one-lane classes only
-            err = a.fp32 ? (sph ? launch_eri<LI, LJ, k, l, true, float>(b) : cudaErrorInvalidValue)
-                         : launch_eri<LI, LJ, k, l, false>(b);
+          if (a.fp32) {
+            err = sph ? launch_eri<LI, LJ, k, l, true, float>(a) : cudaErrorInvalidValue;
+            done = true;
+          } else if (!sph) {
+            err = launch_eri<LI, LJ, k, l, false>(a);
             done = true;
           }
           if constexpr (s1 != s0 || s1 > 1) {
@@ -186,11 +170,7 @@ cudaError_t dispatch_lij(int lk, int ll, bool sph, const LaunchArgs& a) {
               done = true;
             }
           }
-          if (!done) {
-            LaunchArgs b = a;
-            if (!(s0 == 1 && a.variant == 12)) b.queue = nullptr;  // the work queue: variant 12 only
-            err = launch_eri<LI, LJ, k, l, true>(b);
-          }
+          if (!done) err = launch_eri<LI, LJ, k, l, true>(a);
         }
       }
     });

@@ -166,7 +166,7 @@ cudaError_t launch_class(int li, int lj, int lk, int ll, bool sph, const Quartet
                          const ShellPair* pairs, const PrimPair* prims, double* out, OutStrides st,
                          double expcutoff, const RysTable& rys, cudaStream_t stream, bool fp32 = false,
                          double prim_eps = 0.0, int variant = 0, const double* rootbuf = nullptr,
-                         const long long* rootbase = nullptr, int* queue = nullptr);
+                         const long long* rootbase = nullptr);
 // Learned Rys roots (rysnet.cu) of order n at count device points: out[p*2n + f], status[p]
 // (0 refined, 1 table fallback, 2 closed form), asynchronous on stream.
 cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, const double* d_x, long long count,
@@ -174,10 +174,8 @@ cudaError_t rys_learned_eval(const float* d_params, const RysTable& rys, int n, 
 // Lanes per quartet of a launch-shape variant (0 = default shape); variants that do not apply
 // (cartesian or FP32 classes, unknown ids) report the default shape.
 int variant_lanes(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-// true when the launch of this class in this variant takes a device work-queue counter
-bool variant_uses_queue(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
 // Distinct launch shape of a variant (lanes and register cap), for telling variants apart.
 int variant_shape(int li, int lj, int lk, int ll, bool sph, bool fp32, int variant);
-constexpr int kLaunchVariants = 13;
+constexpr int kLaunchVariants = 12;
 
 }  // namespace cintx

@@ -120,9 +120,6 @@ struct CintxPlan {
   QuartetRec* d_recs = nullptr;    // explicit: all records; screened: one chunk's records
   long long rec_capacity = 0;
   char* d_tile_pool = nullptr;     // screened: every tile's rows, cols, prefix and colstart arrays
-  // work-queue counters of persistent-grid launches (variant 12): one per stream the plan launches on
-  int* d_queue = nullptr;
-  std::vector<cudaStream_t> queue_streams;
   std::vector<QuartetRec> h_recs;  // explicit plans keep a host copy for chunk_quartets
   std::vector<int> h_tuples;       // explicit: requested tuples (4 per record, -1 for unit)
   CintxPlanStats stats{};
@@ -158,9 +155,6 @@ void free_plan_device(CintxPlan* p) {
   p->d_recs = nullptr;
   if (p->d_tile_pool) cudaFree(p->d_tile_pool);  // the tiles' arrays live in it
   p->d_tile_pool = nullptr;
-  if (p->d_queue) cudaFree(p->d_queue);
-  p->d_queue = nullptr;
-  p->queue_streams.clear();
   for (Tile& t : p->tiles) {
     t.d_colstart = nullptr;
     t.d_rows = t.d_cols = nullptr;
@@ -242,9 +236,14 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
       return std::tie(li, lj, lk, ll, s0, s1, s2, s3) < std::tie(o.li, o.lj, o.lk, o.ll, o.s0, o.s1, o.s2, o.s3);
     }
   };
-  std::map<GKey, std::vector<QuartetRec>> groups;
-  std::map<GKey, std::vector<int>> group_tuples;
-  std::map<GKey, double> group_flops;
+  struct Group {
+    std::vector<QuartetRec> recs;
+    std::vector<int> tuples;
+    double flops = 0;
+  };
+  std::map<GKey, Group> groups;
+  GKey last_key{};
+  Group* last = nullptr;  // consecutive tuples mostly share a group: one map lookup per change
   long long off = 0;
   double flops = 0;
   long long nprimq = 0;
@@ -343,14 +342,18 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
             long long o2 = off;
             for (int a = 0; a < 4; ++a) o2 += (long long)cs[a] * ne[a] * ast[a];
             r.out = o2;
-            groups[k].push_back(r);
-            for (int a = 0; a < 4; ++a) group_tuples[k].push_back(rs[a]);
+            if (!last || last_key < k || k < last_key) {
+              last = &groups[k];
+              last_key = k;
+            }
+            last->recs.push_back(r);
+            for (int a = 0; a < 4; ++a) last->tuples.push_back(rs[a]);
             const long long npq = (long long)o->pair_nprim[r.pij] * o->pair_nprim[r.pkl];
             nprimq += npq;
             const double fq = npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
                               flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
             flops += fq;
-            group_flops[k] += fq;
+            last->flops += fq;
           }
     off += blk;
   }
@@ -368,13 +371,12 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     sg.st.s3 = kv.first.s3;
     sg.expcutoff = cutoff;
     sg.rec0 = rec0;
-    sg.nrec = (long long)kv.second.size();
+    sg.nrec = (long long)kv.second.recs.size();
     sg.out_off = 0;
-    sg.flops = group_flops[kv.first];
+    sg.flops = kv.second.flops;
     ch.segs.push_back(sg);
-    p->h_recs.insert(p->h_recs.end(), kv.second.begin(), kv.second.end());
-    auto& tu = group_tuples[kv.first];
-    p->h_tuples.insert(p->h_tuples.end(), tu.begin(), tu.end());
+    p->h_recs.insert(p->h_recs.end(), kv.second.recs.begin(), kv.second.recs.end());
+    p->h_tuples.insert(p->h_tuples.end(), kv.second.tuples.begin(), kv.second.tuples.end());
     rec0 += sg.nrec;
   }
   ch.out_size = off;
@@ -398,22 +400,6 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   p->stats.device_bytes = (int64_t)(sizeof(QuartetRec) * rec0);
   *plan = p;
   return CINTX_STATUS_SUCCESS;
-}
-
-constexpr int kQueueSlots = 64;
-
-// The plan's work-queue counter for launches on `stream` (allocated on first use; a plan about to
-// be captured into a graph allocates it before the capture starts), or nullptr.
-static int* queue_slot(CintxPlan* p, cudaStream_t stream) {
-  if (!p->d_queue && cudaMalloc(&p->d_queue, sizeof(int) * kQueueSlots) != cudaSuccess) {
-    p->d_queue = nullptr;
-    return nullptr;
-  }
-  for (size_t i = 0; i < p->queue_streams.size(); ++i)
-    if (p->queue_streams[i] == stream) return p->d_queue + i;
-  if ((int)p->queue_streams.size() >= kQueueSlots) return nullptr;
-  p->queue_streams.push_back(stream);
-  return p->d_queue + (p->queue_streams.size() - 1);
 }
 
 static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStream_t stream, DeviceState* ds,
@@ -447,27 +433,13 @@ static int run_segment(CintxPlan* p, const Segment& sg, double* out_dev, cudaStr
     recs = dst;
     nrec = sg.t1 - sg.t0;
   }
-  // persistent-grid launches take a work-queue counter, zeroed in stream order before each launch
-  int* queue = nullptr;
-  if (variant_uses_queue(sg.li, sg.lj, sg.lk, sg.ll, p->sph, sg.fp32, sg.variant)) {
-    queue = queue_slot(p, stream);
-    if (!queue) {
-      set_error(CINTX_STATUS_ALLOCATION_FAILED, "work-queue counter unavailable");
-      return CINTX_STATUS_ALLOCATION_FAILED;
-    }
-  }
   // the kernels take an int count; split very large segments
   for (long long r0 = 0; r0 < nrec; r0 += 1LL << 30) {
     const int nr = (int)std::min<long long>(nrec - r0, 1LL << 30);
     const bool rb = p->d_rootbuf && sg.tile == -1;  // learned roots: explicit plans only
-    if (queue && cudaMemsetAsync(queue, 0, sizeof(int), stream) != cudaSuccess) {
-      set_error(CINTX_STATUS_EXECUTION_FAILED, "work-queue reset failed");
-      return CINTX_STATUS_EXECUTION_FAILED;
-    }
     cudaError_t e = launch_class(sg.li, sg.lj, sg.lk, sg.ll, p->sph, recs + r0, nr, o->d_pairs, o->d_prims,
                                  out_dev + sg.out_off, sg.st, sg.expcutoff, ds->rys, stream, sg.fp32, sg.prim_eps,
-                                 sg.variant, rb ? p->d_rootbuf : nullptr, rb ? p->d_rootbase + sg.rec0 + r0 : nullptr,
-                                 queue);
+                                 sg.variant, rb ? p->d_rootbuf : nullptr, rb ? p->d_rootbase + sg.rec0 + r0 : nullptr);
     if (e != cudaSuccess) {
       set_error(CINTX_STATUS_EXECUTION_FAILED, std::string("kernel launch failed: ") + cudaGetErrorString(e));
       return CINTX_STATUS_EXECUTION_FAILED;
@@ -1261,12 +1233,6 @@ int cintx_plan_graph_build(CintxPlan* p, const int64_t* chunks, int64_t n, doubl
     p->events.push_back(e);
   }
   cudaStream_t origin = p->branches[0];
-  // the work-queue counters are allocated here: no allocation may happen inside the capture
-  if (!p->d_queue && cudaMalloc(&p->d_queue, sizeof(int) * kQueueSlots) != cudaSuccess) {
-    p->d_queue = nullptr;
-    set_error(CINTX_STATUS_ALLOCATION_FAILED, "work-queue counters could not be allocated");
-    return CINTX_STATUS_ALLOCATION_FAILED;
-  }
   if (cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     set_error(CINTX_STATUS_EXECUTION_FAILED, "stream capture could not start");
     return CINTX_STATUS_EXECUTION_FAILED;

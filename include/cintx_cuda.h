@@ -310,7 +310,7 @@ CINTX_API int cintx_plan_use_tuned_shapes(CintxPlan *plan);
  * to apply without tuning again.  Import returns a status code. */
 CINTX_API int cintx_tuned_shapes_export(int *records, int cap);
 CINTX_API int cintx_tuned_shapes_import(const int *records, int n);
-/* Sets the launch-shape variant (0..12) of every segment, for tests and tuning scripts; a class
+/* Sets the launch-shape variant (0..11) of every segment, for tests and tuning scripts; a class
  * that the variant does not apply to runs its default shape.  Returns the number of segments
  * changed (or -1).  A graph captured earlier is released when anything changed. */
 CINTX_API int cintx_plan_set_shape(CintxPlan *plan, int variant);

@@ -246,9 +246,8 @@ def test_autotuned_launch_shapes_give_the_same_integrals(cx):
 
 def test_every_launch_shape_gives_the_same_integrals(cx):
     """Each launch-shape variant (lane counts, register caps, the sliced shapes whose lanes sit in
-    separate warps, the cooperative shapes with split horizontal transfers, the persistent
-    work-queue grid of the one-lane classes) run on every class of an s/p/d/f molecule matches the
-    default shape."""
+    separate warps, the cooperative shapes with split horizontal transfers) run on every class of an
+    s/p/d/f molecule matches the default shape."""
     mol = M.random_molecule("spdf10", 11, 10, 9.0, with_f=True)
     import torch
     with cx.Optimizer(mol.atm, mol.bas, mol.env) as opt:
@@ -257,7 +256,7 @@ def test_every_launch_shape_gives_the_same_integrals(cx):
         s = torch.cuda.current_stream().cuda_stream
         buf = torch.empty(st.max_chunk_doubles, dtype=torch.float64, device="cuda")
         outs = {}
-        for v in range(13):
+        for v in range(12):
             assert plan.set_shape(v) >= 0
             res = []
             for c in range(st.nchunks):
@@ -267,17 +266,17 @@ def test_every_launch_shape_gives_the_same_integrals(cx):
                 res.append(buf[:plan.chunk_size(c)].cpu().numpy())
             outs[v] = np.concatenate(res)
         assert np.abs(outs[0]).max() > 0
-        for v in range(1, 13):
+        for v in range(1, 12):
             assert close(outs[v], outs[0]), v
         with pytest.raises(cx.CintxError):
-            plan.set_shape(13)
+            plan.set_shape(12)
         plan.close()
 
 
 def test_f_shell_classes_match_libcint_in_every_shape(cx):
     """50 quartets of every f-containing class of the 120-atom molecule (the classes of the
     headline sweep, in random index orders) against libcint at the parity rule, in each launch
-    shape the autotuner can pick (variants 0..12) and in the shapes it picks for them."""
+    shape the autotuner can pick (variants 0..11) and in the shapes it picks for them."""
     mol = M.mol120()
     g = np.load(os.path.join(GOLD, "libcint_mol120f.npz"))
     tup, ref = g["int2e_sph_tuples"], g["int2e_sph_values"]
@@ -290,7 +289,7 @@ def test_f_shell_classes_match_libcint_in_every_shape(cx):
         buf = torch.empty(n, dtype=torch.float64, device="cuda")
         s = torch.cuda.current_stream().cuda_stream
         lanes = set()
-        for v in list(range(13)) + ["tuned"]:
+        for v in list(range(12)) + ["tuned"]:
             if v == "tuned":
                 plan.autotune(buf.data_ptr(), chunk=0, stream=s, reps=1)
             else:
