@@ -228,6 +228,22 @@ __device__ __forceinline__ void quartet_sync(int group) {
   }
 }
 
+// e[j][a] = C(j, a) x^(j - a) for a <= j <= N (zero above the diagonal), by Pascal's rule
+// e[j][a] = e[j-1][a-1] + x e[j-1][a]: the binomial weights of the horizontal transfer come out of
+// multiply-adds on registers, with no integer binomial evaluated in the unrolled loops.
+template <int N, class R>
+__device__ __forceinline__ void pascal_powers(R (&e)[N + 1][N + 1], R x) {
+#pragma unroll
+  for (int j = 0; j <= N; ++j)
+#pragma unroll
+    for (int a = 0; a <= N; ++a) e[j][a] = (R)0;
+  e[0][0] = (R)1;
+#pragma unroll
+  for (int j = 1; j <= N; ++j)
+#pragma unroll
+    for (int a = 0; a <= j; ++a) e[j][a] = (a > 0 ? e[j - 1][a - 1] : (R)0) + (a < j ? x * e[j - 1][a] : (R)0);
+}
+
 // 2D recurrence for one (axis, root) followed by the horizontal transfers; writes
 // I[i + NI*(j + NJ*(k + NK*l))] to dst (stride 1).
 template <int LI, int LJ, int LK, int LL, class R = double>
@@ -249,29 +265,32 @@ __device__ __forceinline__ void vrr_hrr(R* __restrict__ dst, R g00, R c00, R c0p
       G[n][m] = v;
     }
   }
-  R abp[LJ + 1], cdp[LL + 1];
-  abp[0] = (R)1;
+  R ej[LJ + 1][LJ + 1], el[LL + 1][LL + 1];
+  pascal_powers<LJ, R>(ej, ab);
+  pascal_powers<LL, R>(el, cd);
+  // two stages: T(i, j, m) = sum_a e_j[a] G(i+a, m), then I(i, j, k, l) = sum_b e_l[b] T(i, j, k+b)
 #pragma unroll
-  for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
-  cdp[0] = (R)1;
+  for (int j = 0; j <= LJ; ++j)
 #pragma unroll
-  for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
+    for (int i = 0; i <= LI; ++i) {
+      R T[NKL];
 #pragma unroll
-  for (int l = 0; l <= LL; ++l)
+      for (int m = 0; m < NKL; ++m) {
+        R v = (R)0;
 #pragma unroll
-    for (int k = 0; k <= LK; ++k)
+        for (int a = 0; a <= j; ++a) v += ej[j][a] * G[i + a][m];
+        T[m] = v;
+      }
 #pragma unroll
-      for (int j = 0; j <= LJ; ++j)
+      for (int l = 0; l <= LL; ++l)
 #pragma unroll
-        for (int i = 0; i <= LI; ++i) {
+        for (int k = 0; k <= LK; ++k) {
           R v = (R)0;
 #pragma unroll
-          for (int a = 0; a <= j; ++a)
-#pragma unroll
-            for (int b = 0; b <= l; ++b)
-              v += (R)(binom(j, a) * binom(l, b)) * abp[j - a] * cdp[l - b] * G[i + a][k + b];
+          for (int b = 0; b <= l; ++b) v += el[l][b] * T[k + b];
           dst[i + NI * (j + NJ * (k + NK * l))] = v;
         }
+    }
 }
 
 // Shared-memory version for the multi-lane path: the 2D table lives in gs[n*NKL + m]; the
@@ -301,13 +320,9 @@ __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict_
       gs[n * NKL + m] = v;
     }
   }
-  R abp[LJ + 1], cdp[LL + 1];
-  abp[0] = (R)1;
-#pragma unroll
-  for (int t = 1; t <= LJ; ++t) abp[t] = abp[t - 1] * ab;
-  cdp[0] = (R)1;
-#pragma unroll
-  for (int t = 1; t <= LL; ++t) cdp[t] = cdp[t - 1] * cd;
+  R ej[LJ + 1][LJ + 1], el[LL + 1][LL + 1];
+  pascal_powers<LJ, R>(ej, ab);
+  pascal_powers<LL, R>(el, cd);
   for (int i = NPARTS > 1 ? part : 0; i <= LI; i += NPARTS) {
 #pragma unroll
     for (int j = 0; j <= LJ; ++j) {
@@ -316,7 +331,7 @@ __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict_
       for (int m = 0; m < NKL; ++m) {
         R v = (R)0;
 #pragma unroll
-        for (int a = 0; a <= j; ++a) v += (R)binom(j, a) * abp[j - a] * gs[(i + a) * NKL + m];
+        for (int a = 0; a <= j; ++a) v += ej[j][a] * gs[(i + a) * NKL + m];
         T[m] = v;
       }
 #pragma unroll
@@ -325,7 +340,7 @@ __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict_
         for (int k = 0; k <= LK; ++k) {
           R v = (R)0;
 #pragma unroll
-          for (int b = 0; b <= l; ++b) v += (R)binom(l, b) * cdp[l - b] * T[k + b];
+          for (int b = 0; b <= l; ++b) v += el[l][b] * T[k + b];
           dst[i + NI * (j + NJ * (k + NK * l))] = v;
         }
     }

@@ -129,26 +129,22 @@ __device__ __forceinline__ void hrr_jl(double* __restrict__ dst, const double* _
                                        double ab, double cd) {
   constexpr int NKL = LK + LL + 1;
   constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
-  double ca[LJ + 1], cb[LL + 1];
-  // ca[a] = C(j, a) ab^(j - a) for a <= j, else 0 (compile-time loops, runtime selects)
+  // ca[a] = C(j, a) ab^(j - a) for a <= j, else 0: row j of the Pascal table (runtime j: selects)
+  double ej[LJ + 1][LJ + 1], el[LL + 1][LL + 1], ca[LJ + 1], cb[LL + 1];
+  pascal_powers<LJ, double>(ej, ab);
+  pascal_powers<LL, double>(el, cd);
 #pragma unroll
   for (int a = 0; a <= LJ; ++a) {
-    double v = 0.0, p = 1.0;
+    double v = 0.0;
 #pragma unroll
-    for (int jj = a; jj <= LJ; ++jj) {  // p = ab^(jj - a)
-      if (jj == j) v = (double)binom(jj, a) * p;
-      p *= ab;
-    }
+    for (int jj = a; jj <= LJ; ++jj) v = jj == j ? ej[jj][a] : v;
     ca[a] = v;
   }
 #pragma unroll
   for (int b = 0; b <= LL; ++b) {
-    double v = 0.0, p = 1.0;
+    double v = 0.0;
 #pragma unroll
-    for (int l2 = b; l2 <= LL; ++l2) {
-      if (l2 == l) v = (double)binom(l2, b) * p;
-      p *= cd;
-    }
+    for (int l2 = b; l2 <= LL; ++l2) v = l2 == l ? el[l2][b] : v;
     cb[b] = v;
   }
 #pragma unroll

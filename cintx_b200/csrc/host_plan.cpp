@@ -241,121 +241,177 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     std::vector<int> tuples;
     double flops = 0;
   };
-  std::map<GKey, Group> groups;
-  GKey last_key{};
-  Group* last = nullptr;  // consecutive tuples mostly share a group: one map lookup per change
-  long long off = 0;
-  double flops = 0;
-  long long nprimq = 0;
-  for (int64_t q = 0; q < n; ++q) {
+  // 1. requested shells and block sizes (serial; the first bad shell index ends the plan)
+  auto requested = [&](int64_t q, int (&rs)[4], bool (&unit)[4]) {
     const int* s = shls + q * nsh;
-    int rs[4];
-    bool unit[4] = {false, false, false, false};
+    for (int x = 0; x < 4; ++x) unit[x] = false;
     if (family == CINTX_INT2E) {
-      for (int a = 0; a < 4; ++a) rs[a] = s[a];
+      for (int x = 0; x < 4; ++x) rs[x] = s[x];
     } else if (family == CINTX_INT3C2E) {
       rs[0] = s[0]; rs[1] = s[1]; rs[2] = s[2]; rs[3] = -1; unit[3] = true;
     } else {
       rs[0] = s[0]; rs[1] = -1; rs[2] = s[1]; rs[3] = -1; unit[1] = unit[3] = true;
     }
-    int l[4], nc[4], ne[4];
-    for (int a = 0; a < 4; ++a) {
-      if (unit[a]) {
-        l[a] = 0; nc[a] = 1; ne[a] = 1;
-        continue;
-      }
-      if (rs[a] < 0 || rs[a] >= B.nbas) {
-        delete p;
-        set_error(CINTX_STATUS_INVALID_INPUT, "shell index out of range in tuple " + std::to_string(q));
-        return CINTX_STATUS_INVALID_INPUT;
-      }
-      l[a] = B.sh[rs[a]].l;
-      nc[a] = B.sh[rs[a]].nctr;
-      ne[a] = nsph_or_cart(l[a], p->sph);
-    }
-    long long counts[4], ast[4];
+  };
+  std::vector<long long> toff((size_t)n + 1, 0);
+  int64_t bad_shell = n;  // first tuple with a shell index out of range
+  for (int64_t q = 0; q < n; ++q) {
+    int rs[4];
+    bool unit[4];
+    requested(q, rs, unit);
     long long blk = 1;
-    for (int a = 0; a < 4; ++a) counts[a] = (long long)nc[a] * ne[a];
-    {
-      long long st = 1;
-      for (int a = 0; a < 4; ++a) {
-        ast[a] = unit[a] ? 0 : st;
-        if (!unit[a]) st *= counts[a];
-      }
-      blk = st;
+    for (int x = 0; x < 4 && bad_shell == n; ++x) {
+      if (unit[x]) continue;
+      if (rs[x] < 0 || rs[x] >= B.nbas) bad_shell = q;
+      else blk *= (long long)B.sh[rs[x]].nctr * nsph_or_cart(B.sh[rs[x]].l, p->sph);
     }
-    if (offsets_out) offsets_out[q] = off;
-    for (int c3 = 0; c3 < nc[3]; ++c3)
-      for (int c2 = 0; c2 < nc[2]; ++c2)
-        for (int c1 = 0; c1 < nc[1]; ++c1)
-          for (int c0 = 0; c0 < nc[0]; ++c0) {
-            const int cs[4] = {c0, c1, c2, c3};
-            int v[4];
-            for (int a = 0; a < 4; ++a) v[a] = unit[a] ? -1 : B.sh[rs[a]].vbase + cs[a];
-            // pair ids with their table orientation
-            auto pair_of = [&](int x, int y, int& id, bool& x_first) {
-              if (y < 0) {
-                id = o->npairs + x;
-                x_first = true;
-              } else if (x < 0) {
-                id = o->npairs + y;
-                x_first = false;
-              } else {
-                id = pair_index(x, y);
-                x_first = (o->pair_a[id] == x);
+    if (bad_shell != n) break;
+    toff[q + 1] = toff[q] + blk;
+  }
+  // 2. records per kernel class: host threads over tuple ranges (each its own groups, joined in
+  // tuple order below, so the records of a class keep the order of the list)
+  struct Part {
+    std::map<GKey, Group> groups;
+    double flops = 0;
+    long long nprimq = 0;
+    int64_t bad_pair = -1;  // first tuple needing a pair the optimizer does not hold
+  };
+  const int64_t nok = bad_shell;
+  const int nthr = nok >= 65536 ? (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
+  std::vector<Part> parts(nthr);
+  auto work = [&](int t) {
+    Part& P = parts[t];
+    GKey last_key{};
+    Group* last = nullptr;  // consecutive tuples mostly share a group: one map lookup per change
+    const int64_t q0 = nok * t / nthr, q1 = nok * (t + 1) / nthr;
+    for (int64_t q = q0; q < q1; ++q) {
+      int rs[4];
+      bool unit[4];
+      requested(q, rs, unit);
+      int l[4], nc[4], ne[4];
+      for (int x = 0; x < 4; ++x) {
+        l[x] = unit[x] ? 0 : B.sh[rs[x]].l;
+        nc[x] = unit[x] ? 1 : B.sh[rs[x]].nctr;
+        ne[x] = unit[x] ? 1 : nsph_or_cart(l[x], p->sph);
+      }
+      long long ast[4];
+      {
+        long long st = 1;
+        for (int x = 0; x < 4; ++x) {
+          ast[x] = unit[x] ? 0 : st;
+          if (!unit[x]) st *= (long long)nc[x] * ne[x];
+        }
+      }
+      const long long off = toff[q];
+      for (int c3 = 0; c3 < nc[3]; ++c3)
+        for (int c2 = 0; c2 < nc[2]; ++c2)
+          for (int c1 = 0; c1 < nc[1]; ++c1)
+            for (int c0 = 0; c0 < nc[0]; ++c0) {
+              const int cs[4] = {c0, c1, c2, c3};
+              int v[4];
+              for (int x = 0; x < 4; ++x) v[x] = unit[x] ? -1 : B.sh[rs[x]].vbase + cs[x];
+              // pair ids with their table orientation
+              auto pair_of = [&](int x, int y, int& id, bool& x_first) {
+                if (y < 0) {
+                  id = o->npairs + x;
+                  x_first = true;
+                } else if (x < 0) {
+                  id = o->npairs + y;
+                  x_first = false;
+                } else {
+                  id = pair_index(x, y);
+                  x_first = (o->pair_a[id] == x);
+                }
+              };
+              if ((v[0] >= 0 && v[1] >= 0 && std::max(v[0], v[1]) >= o->npv) ||
+                  (v[2] >= 0 && v[3] >= 0 && std::max(v[2], v[3]) >= o->npv)) {
+                P.bad_pair = q;
+                return;
               }
-            };
-            if ((v[0] >= 0 && v[1] >= 0 && std::max(v[0], v[1]) >= o->npv) ||
-                (v[2] >= 0 && v[3] >= 0 && std::max(v[2], v[3]) >= o->npv)) {
-              delete p;
-              set_error(CINTX_STATUS_INVALID_INPUT, "tuple " + std::to_string(q) +
-                                                        " needs a shell pair this optimizer does not hold");
-              return CINTX_STATUS_INVALID_INPUT;
+              int id1, id2;
+              bool f1, f2;
+              pair_of(v[0], v[1], id1, f1);
+              pair_of(v[2], v[3], id2, f2);
+              const int l1a = o->pair_la[id1], l1b = o->pair_lb[id1];
+              const int l2a = o->pair_la[id2], l2b = o->pair_lb[id2];
+              const bool swap = (l2a > l1a) || (l2a == l1a && l2b > l1b);
+              int src[4];
+              const int p1[2] = {f1 ? 0 : 1, f1 ? 1 : 0};
+              const int p2[2] = {f2 ? 2 : 3, f2 ? 3 : 2};
+              if (!swap) {
+                src[0] = p1[0]; src[1] = p1[1]; src[2] = p2[0]; src[3] = p2[1];
+              } else {
+                src[0] = p2[0]; src[1] = p2[1]; src[2] = p1[0]; src[3] = p1[1];
+              }
+              GKey k;
+              k.li = l[src[0]];
+              k.lj = l[src[1]];
+              k.lk = l[src[2]];
+              k.ll = l[src[3]];
+              k.s0 = ast[src[0]];
+              k.s1 = ast[src[1]];
+              k.s2 = ast[src[2]];
+              k.s3 = ast[src[3]];
+              QuartetRec r;
+              r.pij = swap ? id2 : id1;
+              r.pkl = swap ? id1 : id2;
+              long long o2 = off;
+              for (int x = 0; x < 4; ++x) o2 += (long long)cs[x] * ne[x] * ast[x];
+              r.out = o2;
+              if (!last || last_key < k || k < last_key) {
+                last = &P.groups[k];
+                last_key = k;
+              }
+              last->recs.push_back(r);
+              for (int x = 0; x < 4; ++x) last->tuples.push_back(rs[x]);
+              const long long npq = (long long)o->pair_nprim[r.pij] * o->pair_nprim[r.pkl];
+              P.nprimq += npq;
+              const double fq = npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
+                                flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
+              P.flops += fq;
+              last->flops += fq;
             }
-            int id1, id2;
-            bool f1, f2;
-            pair_of(v[0], v[1], id1, f1);
-            pair_of(v[2], v[3], id2, f2);
-            const int l1a = o->pair_la[id1], l1b = o->pair_lb[id1];
-            const int l2a = o->pair_la[id2], l2b = o->pair_lb[id2];
-            const bool swap = (l2a > l1a) || (l2a == l1a && l2b > l1b);
-            int src[4];
-            const int p1[2] = {f1 ? 0 : 1, f1 ? 1 : 0};
-            const int p2[2] = {f2 ? 2 : 3, f2 ? 3 : 2};
-            if (!swap) {
-              src[0] = p1[0]; src[1] = p1[1]; src[2] = p2[0]; src[3] = p2[1];
-            } else {
-              src[0] = p2[0]; src[1] = p2[1]; src[2] = p1[0]; src[3] = p1[1];
-            }
-            GKey k;
-            k.li = l[src[0]];
-            k.lj = l[src[1]];
-            k.lk = l[src[2]];
-            k.ll = l[src[3]];
-            k.s0 = ast[src[0]];
-            k.s1 = ast[src[1]];
-            k.s2 = ast[src[2]];
-            k.s3 = ast[src[3]];
-            QuartetRec r;
-            r.pij = swap ? id2 : id1;
-            r.pkl = swap ? id1 : id2;
-            long long o2 = off;
-            for (int a = 0; a < 4; ++a) o2 += (long long)cs[a] * ne[a] * ast[a];
-            r.out = o2;
-            if (!last || last_key < k || k < last_key) {
-              last = &groups[k];
-              last_key = k;
-            }
-            last->recs.push_back(r);
-            for (int a = 0; a < 4; ++a) last->tuples.push_back(rs[a]);
-            const long long npq = (long long)o->pair_nprim[r.pij] * o->pair_nprim[r.pkl];
-            nprimq += npq;
-            const double fq = npq * flops_per_prim_quartet(k.li, k.lj, k.lk, k.ll) +
-                              flops_c2s(k.li, k.lj, k.lk, k.ll, p->sph);
-            flops += fq;
-            last->flops += fq;
-          }
-    off += blk;
+    }
+  };
+  if (nthr == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthr; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  int64_t bad_pair = -1;
+  for (const Part& P : parts)
+    if (P.bad_pair >= 0) {
+      bad_pair = P.bad_pair;
+      break;
+    }
+  if (bad_pair >= 0 && bad_pair < bad_shell) {
+    delete p;
+    set_error(CINTX_STATUS_INVALID_INPUT,
+              "tuple " + std::to_string(bad_pair) + " needs a shell pair this optimizer does not hold");
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  if (bad_shell < n) {
+    delete p;
+    set_error(CINTX_STATUS_INVALID_INPUT, "shell index out of range in tuple " + std::to_string(bad_shell));
+    return CINTX_STATUS_INVALID_INPUT;
+  }
+  if (offsets_out)
+    for (int64_t q = 0; q < n; ++q) offsets_out[q] = toff[q];
+  const long long off = toff[n];
+  double flops = 0;
+  long long nprimq = 0;
+  std::map<GKey, Group> groups;
+  for (Part& P : parts) {
+    flops += P.flops;
+    nprimq += P.nprimq;
+    for (auto& kv : P.groups) {
+      Group& g = groups[kv.first];
+      g.recs.insert(g.recs.end(), kv.second.recs.begin(), kv.second.recs.end());
+      g.tuples.insert(g.tuples.end(), kv.second.tuples.begin(), kv.second.tuples.end());
+      g.flops += kv.second.flops;
+    }
   }
   Chunk ch;
   long long rec0 = 0;
