@@ -661,7 +661,8 @@ def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
 # launch / its quartets) for the classes that have been the dominant kernel, with the profile
 # summary each figure comes from.
 NCU_TRAFFIC_PER_QUARTET = {
-    "(31|30)": (215.2e6 / 151552, "profiles/eri4c_3130_sliced8_2pass_mol120_spdf.md"),
+    # (dram__bytes_read.sum + dram__bytes_write.sum) of one captured launch / its quartets
+    "(10|00)": ((82505472 + 68205568) / 4594144, "profiles/eri4c_1000_mol120_spdf.md"),
 }
 
 

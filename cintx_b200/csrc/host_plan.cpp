@@ -241,6 +241,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     std::vector<int> tuples;
     double flops = 0;
   };
+  PhaseLog plog("explicit plan");
   // 1. requested shells and block sizes (serial; the first bad shell index ends the plan)
   auto requested = [&](int64_t q, int (&rs)[4], bool (&unit)[4]) {
     const int* s = shls + q * nsh;
@@ -268,6 +269,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     if (bad_shell != n) break;
     toff[q + 1] = toff[q] + blk;
   }
+  plog.mark("block sizes (host)");
   // 2. records per kernel class: host threads over tuple ranges (each its own groups, joined in
   // tuple order below, so the records of a class keep the order of the list)
   struct Part {
@@ -380,6 +382,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     for (int t = 0; t < nthr; ++t) th.emplace_back(work, t);
     for (auto& x : th) x.join();
   }
+  plog.mark("records (host threads)");
   int64_t bad_pair = -1;
   for (const Part& P : parts)
     if (P.bad_pair >= 0) {
@@ -402,20 +405,24 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   const long long off = toff[n];
   double flops = 0;
   long long nprimq = 0;
-  std::map<GKey, Group> groups;
+  // join: the union of the parts' classes in key order; each class's records are its parts'
+  // records in part (= tuple) order, copied once into the plan's host arrays
+  std::map<GKey, std::vector<const Group*>> joined;
+  size_t nrec_total = 0;
   for (Part& P : parts) {
     flops += P.flops;
     nprimq += P.nprimq;
     for (auto& kv : P.groups) {
-      Group& g = groups[kv.first];
-      g.recs.insert(g.recs.end(), kv.second.recs.begin(), kv.second.recs.end());
-      g.tuples.insert(g.tuples.end(), kv.second.tuples.begin(), kv.second.tuples.end());
-      g.flops += kv.second.flops;
+      joined[kv.first].push_back(&kv.second);
+      nrec_total += kv.second.recs.size();
     }
   }
+  p->h_recs.reserve(nrec_total);
+  p->h_tuples.reserve(nrec_total * 4);
+  plog.mark("join");
   Chunk ch;
   long long rec0 = 0;
-  for (auto& kv : groups) {
+  for (auto& kv : joined) {
     Segment sg;
     sg.li = kv.first.li;
     sg.lj = kv.first.lj;
@@ -427,12 +434,16 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     sg.st.s3 = kv.first.s3;
     sg.expcutoff = cutoff;
     sg.rec0 = rec0;
-    sg.nrec = (long long)kv.second.recs.size();
+    sg.nrec = 0;
     sg.out_off = 0;
-    sg.flops = kv.second.flops;
+    sg.flops = 0;
+    for (const Group* g : kv.second) {
+      sg.nrec += (long long)g->recs.size();
+      sg.flops += g->flops;
+      p->h_recs.insert(p->h_recs.end(), g->recs.begin(), g->recs.end());
+      p->h_tuples.insert(p->h_tuples.end(), g->tuples.begin(), g->tuples.end());
+    }
     ch.segs.push_back(sg);
-    p->h_recs.insert(p->h_recs.end(), kv.second.recs.begin(), kv.second.recs.end());
-    p->h_tuples.insert(p->h_tuples.end(), kv.second.tuples.begin(), kv.second.tuples.end());
     rec0 += sg.nrec;
   }
   ch.out_size = off;
@@ -447,6 +458,7 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     }
     cudaMemcpy(p->d_recs, p->h_recs.data(), sizeof(QuartetRec) * rec0, cudaMemcpyHostToDevice);
   }
+  plog.mark("segments, upload");
   p->stats.nquartets = n;
   p->stats.nintegrals = off;
   p->stats.nchunks = 1;
