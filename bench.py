@@ -685,6 +685,24 @@ def roofline_record(per_class, peak64, st, ms_per_step):
             "whole_step_fp64_frac": (st.flops / (ms_per_step * 1e-3) / 1e12) / peak64}
 
 
+def d2h_bandwidth(torch, nbytes=1 << 30, reps=4):
+    """Device-to-host copy bandwidth into page-locked memory (GB/s, best of reps copies of nbytes):
+    the bound of an end-to-end step that brings every integral to the host."""
+    src = torch.empty(nbytes // 8, dtype=torch.float64, device="cuda")
+    dst = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    s = torch.cuda.current_stream()
+    best = 0.0
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        dst.copy_(src, non_blocking=True)
+        e1.record(s)
+        e1.synchronize()
+        best = max(best, nbytes / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del src, dst
+    return best
+
+
 def per_call_latency(cx, reps=3):
     """The drop-in per-call path (int2e_sph with libcint's signature: one block per call, host in
     and out, one device round trip) against libcint's own int2e_sph on the same calls (CPU, one
@@ -920,9 +938,12 @@ def our_arm(args):
         te = max_over_ranks(te_local, device="cuda")
         h2d_all = max_over_ranks(h2d, device="cuda") * world  # every rank uploads the basis and its plan
         d2h_all = st.nintegrals * 8
+        bw = d2h_bandwidth(torch)
         e2e = {"value": st.nintegrals / te / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": int(h2d_all),
                "d2h_bytes_per_step": int(d2h_all), "seconds_per_step": te,
                "phases_s": {k: statistics.mean(v) for k, v in phases.items()},
+               "d2h_gbs_measured": bw, "d2h_bound_gint_s": bw / 8.0 * world,
+               "fraction_of_d2h_bound": (st.nintegrals / te / 1e9) / (bw / 8.0 * world),
                "chunk_doubles": e2e_chunk, "ranks_timed": world,
                "includes": "int2e_optimizer from host atm/bas/env (pair tables, Schwarz passes) + screened "
                            "plan + evaluation + D2H of every integral (each rank its own chunks; a two-chunk "

@@ -367,6 +367,14 @@ __device__ __forceinline__ void load_i_column(double (&v)[NI], const double* __r
   }
 }
 
+// L1 prefetch of the primitive-pair record the next loop iteration reads (one 64-byte line), in the
+// cooperative shapes' primitive loops (in the one-lane path its address arithmetic raised the
+// register count past an occupancy step: (10|00) 8% slower).  No address past the pair's records
+// is prefetched.
+__device__ __forceinline__ void prefetch_prim(const PrimPair* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Per-lane handles on the tuples it owns.
 template <class SH>
 struct LaneTuples {
@@ -632,10 +640,12 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
     } else
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];
+      if (b + 1 < pkl.nprim) prefetch_prim(prims + pkl.prim_off + b + 1);
       const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
       const double qthr = prim_eps / pk.q;  // as in prim_loop_one_lane
       for (int a = 0; a < pij.nprim; ++a) {
         const PrimPair pi = prims[pij.prim_off + a];
+        if (a + 1 < pij.nprim) prefetch_prim(prims + pij.prim_off + a + 1);
         if (pi.q < qthr) break;
         if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
         const double aij = pi.aij, akl = pk.aij;

@@ -204,10 +204,12 @@ __global__ void __launch_bounds__(splitcoop_dims(LI, LJ, LK, LL, ACC).BLOCK, spl
       for (int f = 0; f < NFI; ++f) acc[k][f] = 0.0;
     for (int b = 0; b < pkl.nprim; ++b) {
       const PrimPair pk = prims[pkl.prim_off + b];
+      if (b + 1 < pkl.nprim) prefetch_prim(prims + pkl.prim_off + b + 1);
       const double qcx = pk.px - pkl.ax, qcy = pk.py - pkl.ay, qcz = pk.pz - pkl.az;
       const double qthr = prim_eps / pk.q;  // primitive Schwarz screening, as in eri4c_kernel
       for (int a = 0; a < pij.nprim; ++a) {
         const PrimPair pi = prims[pij.prim_off + a];
+        if (a + 1 < pij.nprim) prefetch_prim(prims + pij.prim_off + a + 1);
         if (pi.q < qthr) break;
         if (pi.cce + pk.cce > expcutoff) continue;  // CINT2e_loop eijcutoff (cint2e.c:700-712)
         const double aij = pi.aij, akl = pk.aij;
