@@ -96,8 +96,9 @@ def parse():
     ap.add_argument("--form", default="tuned", choices=["tuned", "plain"])
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--error-chunks", type=int, default=2)
-    ap.add_argument("--libcint-per-class", type=int, default=2000,
-                    help="quartets per class in the error_vs_libcint sample")
+    ap.add_argument("--libcint-per-class", type=int, default=None,
+                    help="quartets per class in the error_vs_libcint sample (default 2000; mol40_spd: all, "
+                         "so that every integral of that sweep is checked against libcint)")
     ap.add_argument("--no-decomposition", action="store_true",
                     help="skip the FP64-autotuned-shapes and north-star-form comparison sweeps")
     ap.add_argument("--shapes", default=None,
@@ -115,7 +116,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.libcint_per_class is None:
+        args.libcint_per_class = 1 << 40 if args.workload == "mol40_spd" else 2000
+    return args
 
 
 # ------------------------------------------------------------------ clocks
@@ -590,6 +594,15 @@ def class_codes(quartets, lvals):
     return 100 * np.maximum(p1, p2) + np.minimum(p1, p2)
 
 
+def class_codes3(triples, lvals):
+    """Kernel class of each int3c2e triple (a, b, k): the pair (a, b) oriented larger l first and the
+    auxiliary shell as the pair (k, unit), the pair of larger l first (as class_codes)."""
+    l = lvals[triples]
+    p1 = 10 * np.maximum(l[:, 0], l[:, 1]) + np.minimum(l[:, 0], l[:, 1])
+    p2 = 10 * l[:, 2]
+    return 100 * np.maximum(p1, p2) + np.minimum(p1, p2)
+
+
 def code_label(code):
     a, b = divmod(int(code), 100)
     return "(%d%d|%d%d)" % (a // 10, a % 10, b // 10, b % 10)
@@ -608,6 +621,7 @@ def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
     st = plan.stats
     lv = mol.bas[:, 1].astype(np.int64)
     nsph = 2 * lv + 1
+    three = False  # 3-centre plans report tuples (a, b, k, -1): blocks (ab|k), libcint int3c2e_sph
     totals = {}
     for c in range(st.nchunks):
         cls, nq, _ = plan.segments(c)
@@ -618,7 +632,10 @@ def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
     tuples, got = [], []
     for c in range(st.nchunks):
         q = plan.chunk_quartets(c)
-        codes = class_codes(q, lv)
+        if len(q) and (q[:, 3] < 0).all():
+            three = True
+            q = np.ascontiguousarray(q[:, :3])
+        codes = class_codes3(q, lv) if three else class_codes(q, lv)
         prob = np.array([min(1.0, per_class / totals.get(int(k), 1)) for k in range(10000)])
         sel = np.where(rng.random(len(q)) < prob[codes])[0]
         if not len(sel):
@@ -639,7 +656,7 @@ def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
     t2 = time.perf_counter()
     d = np.abs(got - ref)
     ok = (d <= 1e-12) | (d <= 1e-10 * np.abs(ref))
-    codes = class_codes(tuples, lv)
+    codes = class_codes3(tuples, lv) if three else class_codes(tuples, lv)
     per = {}
     blk = np.repeat(codes, np.diff(offs))
     order = np.argsort(blk, kind="stable")
@@ -988,7 +1005,8 @@ def our_arm(args):
             "execution": "one CUDA graph per step (%d kernel classes on %d branches)" % (len(per_class), args.branches)
                          if main_run["graph"] else "direct launches",
             "per_class": {k: {"ms": round(v["ms"], 4), "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3),
-                              "gint_s": round(v["ints"] / (v["ms"] * 1e-3) / 1e9, 2), "quartets": v["quartets"]}
+                              "gint_s": round(v["ints"] / (v["ms"] * 1e-3) / 1e9, 2),
+                              "out_gbs": round(8 * v["ints"] / (v["ms"] * 1e-3) / 1e9, 1), "quartets": v["quartets"]}
                           for k, v in sorted(per_class.items(), key=lambda kv: -kv[1]["ms"])[:16]},
             "profiled_step_ms": sum(v["ms"] for v in per_class.values())}
     if main_run["tuning"] is not None:
@@ -1100,6 +1118,9 @@ def df_arm(args):
                    "reference": "the same chunk with the default launch shapes"}
         q3.close()
         q2.close()
+    err_lib = None
+    if tuned and rank == 0 and world == 1 and not args.no_error and os.path.exists(REF_DRIVER):
+        err_lib = error_vs_libcint(torch, p3, mol, run["rings"][0], stream, args.libcint_per_class, 2029)
     per_class = class_profile(torch, p3, mine3, run["rings"][0], stream)
     peak64 = fp64_peak(cx, torch)
     from types import SimpleNamespace
@@ -1183,6 +1204,8 @@ def df_arm(args):
         line["tuned_over_plain"] = value / plain["value"]
     if err is not None:
         line["error_vs_default_shapes"] = err
+    if err_lib is not None:
+        line["error_vs_libcint"] = err_lib
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
