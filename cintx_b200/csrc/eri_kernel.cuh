@@ -154,7 +154,7 @@ struct EriShape {
   // (multi-lane groups evaluate each root once per group; a per-block copy there costs more
   // occupancy than it saves, measured)
   static constexpr bool STAGE_TABLE = S == 1 && NR <= 3;
-  static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * 2 * NR * (CINTX_RYS_DEG + 1) : 0;
+  static constexpr int TABLE_DOUBLES = STAGE_TABLE ? cintx_rys_xmax(NR) * rys_stage_stride(NR) : 0;
   static constexpr int SMEM_BYTES = Q * B_GROUP + TABLE_DOUBLES * 8;
   static constexpr bool IS_SLICE = SLICE;
   static constexpr int NPASS = PASSES;
@@ -577,9 +577,12 @@ __global__ void __launch_bounds__(EriShape<LI, LJ, LK, LL, SPH, R, ACC, REGS, SL
   R* s_scr = s_g + SH::SM_G;                    // per-lane 2D tables (lanes < 3*NR)
 
   if constexpr (SH::STAGE_TABLE) {
+    // interval blocks of 2*NR*RYS_NC doubles, each placed rys_stage_stride(NR) doubles apart (the
+    // two padding doubles of each interval are never read)
+    constexpr int W = NR * RYS_NC, WP = rys_stage_stride(NR) / 2;  // double2 per block, per stride
     const double2* src = reinterpret_cast<const double2*>(rys.poly[NR]);
     double2* dst = reinterpret_cast<double2*>(smem);
-    for (int i = threadIdx.x; i < SH::TABLE_DOUBLES / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+    for (int i = threadIdx.x; i < cintx_rys_xmax(NR) * W; i += blockDim.x) dst[(i / W) * WP + i % W] = __ldg(src + i);
     __syncthreads();
   }
 

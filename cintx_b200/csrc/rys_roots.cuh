@@ -15,6 +15,12 @@
 // (DEG+1)/2 vector loads.
 constexpr int RYS_NC = CINTX_RYS_DEG + 1;  // coefficients per function (even)
 
+// Doubles per interval of an order-n coefficient block staged in shared memory: the 2n*RYS_NC
+// coefficients plus 2 of padding, so that the interval stride is an odd number of 16-byte units
+// (12n + 1) and the 16-byte loads of lanes reading different intervals spread over the banks
+// (unpadded, stride 12n units: lanes 2 intervals apart, n odd, or any two lanes, n even, collide).
+__host__ __device__ constexpr int rys_stage_stride(int n) { return 2 * n * RYS_NC + 2; }
+
 __device__ __forceinline__ double rys_horner(const double* __restrict__ c, double z) {
   const double2* c2 = reinterpret_cast<const double2*>(c);
   const double2 hi = __ldg(c2 + RYS_NC / 2 - 1);
@@ -66,8 +72,8 @@ __device__ __forceinline__ void rys_all(const RysTable& c_rys, double x, double*
   }
 }
 
-// As rys_all, with the order-N coefficient block (cintx_rys_xmax(N) intervals) staged in shared
-// memory at `tab`; only the large-x limit reads global memory.
+// As rys_all, with the order-N coefficient block (cintx_rys_xmax(N) intervals, rys_stage_stride(N)
+// doubles apart) staged in shared memory at `tab`; only the large-x limit reads global memory.
 template <int N, int F0 = 0, int F1 = 2 * N>
 __device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable& c_rys, double x, double* t2,
                                                double* w) {
@@ -85,7 +91,7 @@ __device__ __forceinline__ void rys_all_staged(const double* tab, const RysTable
   }
   const int i = (int)x;
   const double z = 2.0 * (x - (double)i) - 1.0;
-  const double* c = tab + (size_t)i * 2 * N * RYS_NC;
+  const double* c = tab + (size_t)i * rys_stage_stride(N);
   auto horner = [&](int f) {
     const double2* c2 = reinterpret_cast<const double2*>(c + f * RYS_NC);
     const double2 hi = c2[RYS_NC / 2 - 1];
@@ -118,7 +124,7 @@ __device__ __forceinline__ double rys_fn_staged(const double* tab, const RysTabl
   }
   const int i = (int)x;
   const double z = 2.0 * (x - (double)i) - 1.0;
-  const double2* c2 = reinterpret_cast<const double2*>(tab + ((size_t)i * 2 * N + f) * RYS_NC);
+  const double2* c2 = reinterpret_cast<const double2*>(tab + (size_t)i * rys_stage_stride(N) + f * RYS_NC);
   const double2 hi = c2[RYS_NC / 2 - 1];
   double acc = fma(hi.y, z, hi.x);
 #pragma unroll
