@@ -256,18 +256,40 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
   };
   std::vector<long long> toff((size_t)n + 1, 0);
   int64_t bad_shell = n;  // first tuple with a shell index out of range
-  for (int64_t q = 0; q < n; ++q) {
-    int rs[4];
-    bool unit[4];
-    requested(q, rs, unit);
-    long long blk = 1;
-    for (int x = 0; x < 4 && bad_shell == n; ++x) {
-      if (unit[x]) continue;
-      if (rs[x] < 0 || rs[x] >= B.nbas) bad_shell = q;
-      else blk *= (long long)B.sh[rs[x]].nctr * nsph_or_cart(B.sh[rs[x]].l, p->sph);
+  {
+    // block sizes into toff[q + 1] on host threads over tuple ranges, then one prefix sum
+    const int nb = n >= 65536 ? (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
+    std::vector<int64_t> bad(nb, n);
+    auto sizes = [&](int t) {
+      for (int64_t q = n * t / nb; q < n * (t + 1) / nb; ++q) {
+        int rs[4];
+        bool unit[4];
+        requested(q, rs, unit);
+        long long blk = 1;
+        for (int x = 0; x < 4; ++x) {
+          if (unit[x]) continue;
+          if (rs[x] < 0 || rs[x] >= B.nbas) {
+            bad[t] = q;
+            return;
+          }
+          blk *= (long long)B.sh[rs[x]].nctr * nsph_or_cart(B.sh[rs[x]].l, p->sph);
+        }
+        toff[q + 1] = blk;
+      }
+    };
+    if (nb == 1) {
+      sizes(0);
+    } else {
+      std::vector<std::thread> th;
+      for (int t = 0; t < nb; ++t) th.emplace_back(sizes, t);
+      for (auto& x : th) x.join();
     }
-    if (bad_shell != n) break;
-    toff[q + 1] = toff[q] + blk;
+    for (int t = 0; t < nb; ++t)
+      if (bad[t] < n) {
+        bad_shell = bad[t];
+        break;
+      }
+    for (int64_t q = 0; q < bad_shell; ++q) toff[q + 1] += toff[q];
   }
   plog.mark("block sizes (host)");
   // 2. records per kernel class: host threads over tuple ranges (each its own groups, joined in
@@ -417,11 +439,12 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
       nrec_total += kv.second.recs.size();
     }
   }
-  p->h_recs.reserve(nrec_total);
-  p->h_tuples.reserve(nrec_total * 4);
+  p->h_recs.resize(nrec_total);
+  p->h_tuples.resize(nrec_total * 4);
   plog.mark("join");
   Chunk ch;
   long long rec0 = 0;
+  std::vector<std::pair<const Group*, long long>> copies;  // (part group, first record)
   for (auto& kv : joined) {
     Segment sg;
     sg.li = kv.first.li;
@@ -438,13 +461,29 @@ int cintx_plan_shells(CintxPlan** plan, CINTOpt* optp, int family, const int* sh
     sg.out_off = 0;
     sg.flops = 0;
     for (const Group* g : kv.second) {
+      copies.emplace_back(g, rec0 + sg.nrec);
       sg.nrec += (long long)g->recs.size();
       sg.flops += g->flops;
-      p->h_recs.insert(p->h_recs.end(), g->recs.begin(), g->recs.end());
-      p->h_tuples.insert(p->h_tuples.end(), g->tuples.begin(), g->tuples.end());
     }
     ch.segs.push_back(sg);
     rec0 += sg.nrec;
+  }
+  {
+    // the records and tuples of every part group into place, on host threads
+    std::atomic<size_t> next(0);
+    auto place = [&]() {
+      for (size_t j; (j = next.fetch_add(1)) < copies.size();) {
+        const Group* g = copies[j].first;
+        const long long r = copies[j].second;
+        if (!g->recs.empty()) memcpy(p->h_recs.data() + r, g->recs.data(), sizeof(QuartetRec) * g->recs.size());
+        if (!g->tuples.empty()) memcpy(p->h_tuples.data() + 4 * r, g->tuples.data(), sizeof(int) * g->tuples.size());
+      }
+    };
+    const int nc = copies.size() > 16 ? (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
+    std::vector<std::thread> th;
+    for (int t = 1; t < nc; ++t) th.emplace_back(place);
+    place();
+    for (auto& x : th) x.join();
   }
   ch.out_size = off;
   ch.nrec = rec0;
