@@ -720,6 +720,36 @@ def d2h_bandwidth(torch, nbytes=1 << 30, reps=4):
     return best
 
 
+def ip1_record(cx, torch, plan, mol, n=200_000, seed=91, reps=3):
+    """First-derivative integrals int2e_ip1_sph (three components per block) of a seeded uniform
+    sample of the sweep's quartets through the batched entry point (cintx_ip1_eval: host set-up,
+    kernels, into a device buffer; wall time of the call, best of reps) against libcint 6.1.3's
+    int2e_ip1_sph on the same tuples on all host cores."""
+    from oracle import RefLibcint
+    q = np.unique(plan.sample_quartets(n, seed), axis=0)
+    nd = cx.ip1_len(cx.INT2E, q, mol.bas)
+    buf = torch.empty(nd, dtype=torch.float64, device="cuda")
+    best = 1e300
+    for _ in range(reps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cx.ip1_eval(cx.INT2E, q, mol.atm, mol.bas, mol.env, buf.data_ptr())
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+    got = buf.cpu().numpy()
+    t0 = time.perf_counter()
+    ref, _, _ = RefLibcint().batch(q, mol, ip1=True)
+    t_lib = time.perf_counter() - t0
+    d = np.abs(got - ref)
+    return {"quartets": int(len(q)), "integrals": int(nd), "seconds": best, "gint_s": nd / best / 1e9,
+            "libcint_seconds": t_lib, "libcint_gint_s": nd / t_lib / 1e9, "cores": os.cpu_count(),
+            "max_abs_vs_libcint": float(d.max()),
+            "parity_rule_share": float(((d <= 1e-12) | (d <= 1e-10 * np.abs(ref))).mean()),
+            "what": "int2e_ip1_sph (3 components per block) of a seeded uniform sample of the sweep's quartets: "
+                    "cintx_ip1_eval wall time (host set-up + kernels, output on the device) vs libcint on all "
+                    "host cores, same tuples"}
+
+
 def per_call_latency(cx, reps=3):
     """The drop-in per-call path (int2e_sph with libcint's signature: one block per call, host in
     and out, one device round trip) against libcint's own int2e_sph on the same calls (CPU, one
@@ -905,9 +935,10 @@ def our_arm(args):
     jk = None
     if rank == 0 and world == 1 and not args.no_jk:
         jk = jk_timing(cx, torch, plan, mol, stream, min(args.steps, 5))
-    per_call = None
+    per_call = ip1 = None
     if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):
         per_call = per_call_latency(cx)
+        ip1 = ip1_record(cx, torch, plan, mol)
 
     # end-to-end through the C ABI from host arrays, measured on every rank over its own chunks:
     # optimizer from atm/bas/env, screened plan, evaluation and D2H into page-locked host memory;
@@ -1048,6 +1079,8 @@ def our_arm(args):
         line["jk_build"] = jk
     if per_call is not None:
         line["per_call"] = per_call
+    if ip1 is not None:
+        line["ip1"] = ip1
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu and os.path.exists(REF_DRIVER):

@@ -14,6 +14,7 @@
 #include <map>
 #include <string>
 #include <tuple>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/cintx_cuda.h"
@@ -82,9 +83,11 @@ int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, boo
               int64_t* offsets) {
   const double cutoff = nsh == 4 ? expcutoff_2e(B.env.data()) : expcutoff_3c(B.env.data());
   const double pair_cutoff = opt_mode ? expcutoff_3c(B.env.data()) : cutoff;
-  std::map<std::tuple<int, int, int>, int> pair_id;  // (a, b, derivative) -> id
+  // (a, b, derivative) -> pair id, packed into one 64-bit key (b may be -1: unit pair)
+  std::unordered_map<uint64_t, int> pair_id;
+  pair_id.reserve(1024);
   auto get_pair = [&](int a, int b, bool deriv) {
-    auto key = std::make_tuple(a, b, deriv ? 1 : 0);
+    const uint64_t key = ((uint64_t)(uint32_t)a << 33) | ((uint64_t)(uint32_t)(b + 1) << 1) | (deriv ? 1u : 0u);
     auto it = pair_id.find(key);
     if (it != pair_id.end()) return it->second;
     PairHost ph;
@@ -102,6 +105,19 @@ int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, boo
     return id;
   };
   auto ncomp = [&](int l) { return sph ? 2 * l + 1 : (l + 1) * (l + 2) / 2; };
+  // recurrence centre of each (k, l) pair, computed once per pair (pair_base_first loops over the
+  // primitive exponents)
+  std::unordered_map<uint64_t, bool> kfirst;
+  auto centre_first = [&](int k, int l2) {
+    const uint64_t key = ((uint64_t)(uint32_t)k << 32) | (uint32_t)l2;
+    auto it = kfirst.find(key);
+    if (it != kfirst.end()) return it->second;
+    const bool f = pair_base_first(B, k, l2);
+    kfirst.emplace(key, f);
+    return f;
+  };
+  std::vector<QuartetRec>* last = nullptr;  // consecutive tuples mostly share a group
+  Ip1Work::Key last_key{};
   long long off = 0;
   for (int64_t q = 0; q < n; ++q) {
     const int* s = shls + q * nsh;
@@ -123,7 +139,7 @@ int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, boo
       ne[a] = ncomp(l[a]);
     }
     // kernel axes: (i, j) as requested; (k, l) with the recurrence centre first
-    const bool kf = rs[3] < 0 || pair_base_first(B, rs[2], rs[3]);
+    const bool kf = rs[3] < 0 || centre_first(rs[2], rs[3]);
     const int src[4] = {0, 1, kf ? 2 : 3, kf ? 3 : 2};
     if (!ip1_class_valid(l[0], l[1], l[src[2]], l[src[3]])) {
       set_error(CINTX_STATUS_UNSUPPORTED_API, "derivative integrals are compiled for l <= 3 on the differentiated "
@@ -151,7 +167,11 @@ int ip1_build(const Basis& B, int nsh, const int* shls, int64_t n, bool sph, boo
             r.out = off;
             for (int a = 0; a < 4; ++a) r.out += (long long)cs[a] * ne[a] * ast[a];
             Ip1Work::Key k{l[0], l[1], l[src[2]], l[src[3]], ast[0], ast[1], ast[src[2]], ast[src[3]], st};
-            W.groups[k].push_back(r);
+            if (!last || last_key < k || k < last_key) {
+              last = &W.groups[k];
+              last_key = k;
+            }
+            last->push_back(r);
           }
     off += 3 * st;
   }
