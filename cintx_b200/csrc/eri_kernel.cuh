@@ -293,6 +293,39 @@ __device__ __forceinline__ void vrr_hrr(R* __restrict__ dst, R g00, R c00, R c0p
     }
 }
 
+// The 2D table of one (axis, root) (the vertical recurrence of vrr_hrr, CINTg0_2e_2d g2e.c:272),
+// built in registers one column m at a time (three columns live, every index a compile-time
+// constant) and stored to gt[n * NKL + m].
+template <int NIJ, int NKL, class R>
+__device__ __forceinline__ void vrr_columns(R* __restrict__ gt, R g00, R c00, R c0p, R b10, R b01, R b00) {
+  R c1[NIJ], c2[NIJ];  // columns m - 1 and m - 2
+  c1[0] = g00;
+#pragma unroll
+  for (int n = 1; n < NIJ; ++n) c1[n] = c00 * c1[n - 1] + (n > 1 ? (R)(n - 1) * b10 * c1[n - 2] : (R)0);
+#pragma unroll
+  for (int n = 0; n < NIJ; ++n) {
+    gt[n * NKL] = c1[n];
+    c2[n] = (R)0;
+  }
+#pragma unroll
+  for (int m = 1; m < NKL; ++m) {
+    R c[NIJ];
+#pragma unroll
+    for (int n = 0; n < NIJ; ++n) {
+      R v = c0p * c1[n];
+      if (m > 1) v += (R)(m - 1) * b01 * c2[n];
+      if (n > 0) v += (R)n * b00 * c1[n - 1];
+      c[n] = v;
+    }
+#pragma unroll
+    for (int n = 0; n < NIJ; ++n) {
+      gt[n * NKL + m] = c[n];
+      c2[n] = c1[n];
+      c1[n] = c[n];
+    }
+  }
+}
+
 // Shared-memory version for the multi-lane path: the 2D table lives in gs[n*NKL + m]; the
 // horizontal transfers are unrolled over j and the (k, l) outputs, looped over i.
 // NPARTS > 1: this call writes only the i = part, part + NPARTS, ... rows of the transfers (the
@@ -302,24 +335,7 @@ __device__ __forceinline__ void vrr_hrr_smem(R* __restrict__ dst, R* __restrict_
                                              R b01, R b00, R ab, R cd, int part = 0) {
   constexpr int NIJ = LI + LJ + 1, NKL = LK + LL + 1;
   constexpr int NI = LI + 1, NJ = LJ + 1, NK = LK + 1;
-  {
-    R gm2 = (R)0, gm1 = g00;
-    gs[0] = g00;
-    for (int n = 1; n < NIJ; ++n) {
-      const R g = c00 * gm1 + (R)(n - 1) * b10 * gm2;
-      gs[n * NKL] = g;
-      gm2 = gm1;
-      gm1 = g;
-    }
-  }
-  for (int m = 1; m < NKL; ++m) {
-    for (int n = 0; n < NIJ; ++n) {
-      R v = c0p * gs[n * NKL + m - 1];
-      if (m > 1) v += (R)(m - 1) * b01 * gs[n * NKL + m - 2];
-      if (n > 0) v += (R)n * b00 * gs[(n - 1) * NKL + m - 1];
-      gs[n * NKL + m] = v;
-    }
-  }
+  vrr_columns<NIJ, NKL, R>(gs, g00, c00, c0p, b10, b01, b00);
   R ej[LJ + 1][LJ + 1], el[LL + 1][LL + 1];
   pascal_powers<LJ, R>(ej, ab);
   pascal_powers<LL, R>(el, cd);

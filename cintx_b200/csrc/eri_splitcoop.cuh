@@ -86,39 +86,6 @@ __host__ __device__ constexpr int splitcoop_violation() {
   return 0;
 }
 
-// The 2D table of one (axis, root) (the vertical recurrence of vrr_hrr, CINTg0_2e_2d g2e.c:272),
-// built one column m at a time and stored to gt[n * NKL + m].
-template <int NIJ, int NKL>
-__device__ __forceinline__ void vrr_columns(double* __restrict__ gt, double g00, double c00, double c0p,
-                                            double b10, double b01, double b00) {
-  double c1[NIJ], c2[NIJ];  // columns m - 1 and m - 2
-  c1[0] = g00;
-#pragma unroll
-  for (int n = 1; n < NIJ; ++n) c1[n] = c00 * c1[n - 1] + (n > 1 ? (double)(n - 1) * b10 * c1[n - 2] : 0.0);
-#pragma unroll
-  for (int n = 0; n < NIJ; ++n) {
-    gt[n * NKL] = c1[n];
-    c2[n] = 0.0;
-  }
-#pragma unroll
-  for (int m = 1; m < NKL; ++m) {
-    double c[NIJ];
-#pragma unroll
-    for (int n = 0; n < NIJ; ++n) {
-      double v = c0p * c1[n];
-      if (m > 1) v += (double)(m - 1) * b01 * c2[n];
-      if (n > 0) v += (double)n * b00 * c1[n - 1];
-      c[n] = v;
-    }
-#pragma unroll
-    for (int n = 0; n < NIJ; ++n) {
-      gt[n * NKL + m] = c[n];
-      c2[n] = c1[n];
-      c1[n] = c[n];
-    }
-  }
-}
-
 // Horizontal transfers of one (axis, root) for one (j, l):
 //   I(i, j, k, l) = sum_a sum_b C(j,a) C(l,b) ab^(j-a) cd^(l-b) G(i+a, k+b)
 // for all i <= LI, k <= LK, from the table gt[n * NKL + m] (closed binomial form of g2e.c:428-694),
@@ -237,8 +204,8 @@ __global__ void __launch_bounds__(splitcoop_dims(LI, LJ, LK, LL, ACC).BLOCK, spl
           const double qc = axis == 0 ? qcx : (axis == 1 ? qcy : qcz);
           const double pq = axis == 0 ? pqx : (axis == 1 ? pqy : pqz);
           const double g00 = axis == 2 ? s_roots[NR + r] * fac : 1.0;
-          vrr_columns<NIJ, NKL>(s_t + task * (NIJ * NKL), g00, pa - rt_aa * akl * pq, qc + rt_aa * aij * pq, b10,
-                                b01, b00);
+          vrr_columns<NIJ, NKL, double>(s_t + task * (NIJ * NKL), g00, pa - rt_aa * akl * pq,
+                                        qc + rt_aa * aij * pq, b10, b01, b00);
         }
         group_sync<S>(group);
         // H: the transfers, one (axis, root, j, l) per task
