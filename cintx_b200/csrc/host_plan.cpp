@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -82,10 +83,14 @@ struct Chunk {
 struct Tile {
   int typeA, typeB;
   int li, lj, lk, ll;
-  std::vector<int> rows, cols;          // pair ids
+  std::vector<int> rows;                // pair ids
+  // column pair ids and the prefix of their primitive-pair counts (size cols+1), shared by every
+  // tile of one column type
+  std::shared_ptr<const std::vector<int>> cols;
+  std::shared_ptr<const std::vector<long long>> cum_np;
   std::vector<long long> row_prefix;    // size rows+1
-  std::vector<long long> cum_np;        // prefix of primitive-pair counts over cols
   std::vector<int> colstart;            // per row: first column (empty: 0 for every row)
+  long long nprimq = -1;                // primitive quartets of the tile (-1: not yet counted)
   bool fp32 = false;                    // evaluated with FP32 recurrences
   bool swap = false;                    // records take (pij, pkl) = (col, row): the kernel's first pair is the col
   OutStrides st{};                      // output strides of the kernel's axes
@@ -1021,7 +1026,7 @@ int cintx_plan_chunk_quartets(const CintxPlan* p, int64_t chunk, int* quartets, 
       for (long long q = sg.t0; q < sg.t1; ++q, ++k) {
         if (k >= cap) return CINTX_STATUS_BUFFER_TOO_SMALL;
         const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
-        const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
+        const int pa = t.rows[row], pb = (*t.cols)[t.col0(row) + q - t.row_prefix[row]];
         const int2 ra = reported_shells(o, pa), rb = reported_shells(o, pb);
         quartets[k * 4 + 0] = ra.x;
         quartets[k * 4 + 1] = ra.y;
@@ -1072,7 +1077,7 @@ int cintx_plan_sample_quartets(const CintxPlan* p, uint64_t seed, int64_t n, int
       const Tile& t = p->tiles[ti];
       const long long q = g - tp[ti];
       const long long row = std::upper_bound(t.row_prefix.begin(), t.row_prefix.end(), q) - t.row_prefix.begin() - 1;
-      const int pa = t.rows[row], pb = t.cols[t.col0(row) + q - t.row_prefix[row]];
+      const int pa = t.rows[row], pb = (*t.cols)[t.col0(row) + q - t.row_prefix[row]];
       const int2 ra = reported_shells(o, pa), rb = reported_shells(o, pb);
       quartets[k * 4 + 0] = ra.x;
       quartets[k * 4 + 1] = ra.y;
@@ -1724,21 +1729,31 @@ static double c2s_amp(int l, bool sph) {
 // Shared tail of the screened planners: flop model, primitive-screening thresholds, chunking at
 // quartet boundaries, per-class merged segments and device upload.  The tiles of p are complete
 // (rows, cols, row_prefix, cum_np, kernel class, strides, swap).
+static long long tile_prim_quartets(const Tile& t, const Opt* o) {
+  const std::vector<long long>& cum = *t.cum_np;
+  long long tp = 0;
+  for (size_t r = 0; r < t.rows.size(); ++r) {
+    const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
+    tp += (long long)o->pair_nprim[t.rows[r]] * (cum[t.col0(r) + cnt] - cum[t.col0(r)]);
+  }
+  return tp;
+}
+
 static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk, double prim_budget,
                            long long nq_total, long long nint_total, long long nq_fp32, CintxPlan** plan) {
+  // tiles of one kernel class next to each other, so that a chunk holds few classes (few
+  // launches when the sweep runs in many small chunks) and a class's records fill large launches
+  std::stable_sort(p->tiles.begin(), p->tiles.end(), [](const Tile& x, const Tile& y) {
+    return std::make_tuple(x.li, x.lj, x.lk, x.ll, x.fp32, x.swap) <
+           std::make_tuple(y.li, y.lj, y.lk, y.ll, y.fp32, y.swap);
+  });
   long long nprimq = 0;
   double flops = 0;
   // flops: per tile class
   {
     // recompute nprim-weighted flops per tile
     for (const Tile& t : p->tiles) {
-      std::vector<long long> cum(t.cols.size() + 1, 0);
-      for (size_t c = 0; c < t.cols.size(); ++c) cum[c + 1] = cum[c] + o->pair_nprim[t.cols[c]];
-      long long tp = 0;
-      for (size_t r = 0; r < t.rows.size(); ++r) {
-        const long long cnt = t.row_prefix[r + 1] - t.row_prefix[r];
-        tp += (long long)o->pair_nprim[t.rows[r]] * (cum[t.col0(r) + cnt] - cum[t.col0(r)]);
-      }
+      const long long tp = t.nprimq >= 0 ? t.nprimq : tile_prim_quartets(t, o);
       nprimq += tp;
       const long long nq = t.row_prefix.back();
       flops += tp * flops_per_prim_quartet(t.li, t.lj, t.lk, t.ll) + nq * flops_c2s(t.li, t.lj, t.lk, t.ll, p->sph);
@@ -1803,7 +1818,7 @@ static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk,
         while (pos < q + take) {
           const long long rend = std::min(t.row_prefix[r + 1], q + take);
           const long long c0 = t.col0(r) + pos - t.row_prefix[r], c1 = t.col0(r) + rend - t.row_prefix[r];
-          fl += (double)o->pair_nprim[t.rows[r]] * (double)(t.cum_np[c1] - t.cum_np[c0]) * fpp;
+          fl += (double)o->pair_nprim[t.rows[r]] * (double)((*t.cum_np)[c1] - (*t.cum_np)[c0]) * fpp;
           pos = rend;
           ++r;
         }
@@ -1823,26 +1838,57 @@ static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk,
   p->rec_capacity = max_recs;
   bool ok = true;
   if (max_recs > 0) ok = cudaMalloc(&p->d_recs, sizeof(QuartetRec) * max_recs) == cudaSuccess;
-  // every tile's arrays in one device allocation and one copy (256-byte aligned slices)
+  // every tile's arrays in one device allocation and one copy (256-byte aligned slices); a
+  // column list shared by several tiles is stored once
+  size_t pool_bytes = 0;
   if (ok && !p->tiles.empty()) {
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    std::map<const std::vector<int>*, size_t> col_at;  // shared column list -> its slice
     size_t total = 0;
-    for (const Tile& t : p->tiles)
-      total += align(sizeof(int) * t.rows.size()) + align(sizeof(int) * t.cols.size()) +
-               align(sizeof(long long) * t.row_prefix.size()) + align(sizeof(int) * t.colstart.size());
+    for (const Tile& t : p->tiles) {
+      total += align(sizeof(int) * t.rows.size()) + align(sizeof(long long) * t.row_prefix.size()) +
+               align(sizeof(int) * t.colstart.size());
+      if (col_at.emplace(t.cols.get(), 0).second) total += align(sizeof(int) * t.cols->size());
+    }
+    pool_bytes = total;
     std::vector<char> img(std::max<size_t>(total, 1));
     std::vector<size_t> at;  // slice offsets: rows, cols, prefix, colstart of each tile
+    struct Copy {
+      const void* src;
+      size_t bytes, pos;
+    };
+    std::vector<Copy> copies;  // filled in on host threads below
     size_t pos = 0;
     auto put = [&](const void* src, size_t bytes) {
       at.push_back(pos);
-      if (bytes) memcpy(img.data() + pos, src, bytes);
+      if (bytes) copies.push_back({src, bytes, pos});
       pos += align(bytes);
     };
+    col_at.clear();
     for (const Tile& t : p->tiles) {
       put(t.rows.data(), sizeof(int) * t.rows.size());
-      put(t.cols.data(), sizeof(int) * t.cols.size());
+      auto it = col_at.find(t.cols.get());
+      if (it == col_at.end()) {
+        put(t.cols->data(), sizeof(int) * t.cols->size());
+        col_at.emplace(t.cols.get(), at.back());
+      } else {
+        at.push_back(it->second);
+      }
       put(t.row_prefix.data(), sizeof(long long) * t.row_prefix.size());
       put(t.colstart.data(), sizeof(int) * t.colstart.size());
+    }
+    {
+      std::atomic<size_t> next(0);
+      auto worker = [&]() {
+        for (size_t j; (j = next.fetch_add(64)) < copies.size();)
+          for (size_t k = j; k < std::min(j + 64, copies.size()); ++k)
+            memcpy(img.data() + copies[k].pos, copies[k].src, copies[k].bytes);
+      };
+      const int nthr = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+      std::vector<std::thread> th;
+      for (int i = 1; i < nthr && (size_t)i * 64 < copies.size(); ++i) th.emplace_back(worker);
+      worker();
+      for (auto& x : th) x.join();
     }
     ok = cudaMalloc(&p->d_tile_pool, std::max<size_t>(total, 256)) == cudaSuccess;
     if (ok) ok = cudaMemcpy(p->d_tile_pool, img.data(), total, cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1934,10 +1980,7 @@ static int finish_screened(CintxPlan* p, Opt* o, double ecut, int64_t max_chunk,
   p->stats.flops = flops;
   p->stats.nquartets_fp32 = nq_fp32;
   {
-    long long db = (long long)sizeof(QuartetRec) * max_recs;
-    for (const Tile& t : p->tiles)
-      db += (long long)(sizeof(int) * (t.rows.size() + t.cols.size()) + sizeof(long long) * t.row_prefix.size());
-    p->stats.device_bytes = db;
+    p->stats.device_bytes = (long long)sizeof(QuartetRec) * max_recs + (long long)pool_bytes;
   }
   *plan = p;
   return CINTX_STATUS_SUCCESS;
@@ -1981,21 +2024,42 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
   int rc = diag_schwarz_2e(o, expcutoff_2e(B.env.data()), Q, -1);
   if (rc) return rc;
   plog.mark("diagonal Schwarz pass");
-  // 2. pair types (la, lb, nprim_a, nprim_b), sorted pairs by decreasing Q
-  std::map<std::tuple<int, int, int, int>, std::vector<int>> types;
+  // 2. pair types (la, lb, nprim_a, nprim_b, work bucket), sorted pairs by decreasing Q.  The
+  // bucket groups pairs by their primitive-pair count after exponent screening (half-octave
+  // steps): a (kl) pair's count is the trip count of each lane's outer primitive loop, so
+  // columns of one type give the lanes of a warp (consecutive columns of a row) equal trip
+  // counts instead of running to the longest lane's.
+  auto work_bucket = [](int n) {
+    int k = 0;
+    while ((2 << k) <= n) ++k;  // 2^k <= n < 2^(k+1)
+    return 2 * k + ((long long)n * n >= (2LL << (2 * k)) ? 1 : 0);
+  };
+  std::map<std::tuple<int, int, int, int, int>, std::vector<int>> types;
   double qmax = 0;
   for (int id = 0; id < np; ++id) qmax = std::max(qmax, Q[id]);
   for (int id = 0; id < np; ++id) {
     if (!(Q[id] * qmax >= cutoff) || o->pair_nprim[id] == 0) continue;
     const int a = o->pair_a[id], b = o->pair_b[id];
-    types[std::make_tuple(o->pair_la[id], o->pair_lb[id], B.sh[a].nprim, B.sh[b].nprim)].push_back(id);
+    types[std::make_tuple(o->pair_la[id], o->pair_lb[id], B.sh[a].nprim, B.sh[b].nprim, work_bucket(o->pair_nprim[id]))]
+        .push_back(id);
   }
-  std::vector<std::vector<int>> tlist;
-  std::vector<std::tuple<int, int, int, int>> tkeys;
+  // per type: its pairs, their Q and their primitive-pair prefix, shared by the type's tiles
+  std::vector<std::shared_ptr<const std::vector<int>>> tlist;
+  std::vector<std::shared_ptr<const std::vector<long long>>> tcum;
+  std::vector<std::vector<double>> tq;
+  std::vector<std::tuple<int, int, int, int, int>> tkeys;
   for (auto& kv : types) {
     std::vector<int> v = kv.second;
     std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return Q[x] > Q[y]; });
-    tlist.push_back(v);
+    std::vector<long long> cum(v.size() + 1, 0);
+    std::vector<double> q(v.size());
+    for (size_t c = 0; c < v.size(); ++c) {
+      cum[c + 1] = cum[c] + o->pair_nprim[v[c]];
+      q[c] = Q[v[c]];
+    }
+    tlist.push_back(std::make_shared<const std::vector<int>>(std::move(v)));
+    tcum.push_back(std::make_shared<const std::vector<long long>>(std::move(cum)));
+    tq.push_back(std::move(q));
     tkeys.push_back(kv.first);
   }
   CintxPlan* p = new CintxPlan();
@@ -2023,12 +2087,9 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
     // equal-l pairs are reported (other, centre): their two axes trade strides
     if (t.li == t.lj) std::swap(t.st.s0, t.st.s1);
     if (t.lk == t.ll) std::swap(t.st.s2, t.st.s3);
-    const std::vector<int>& rows = tlist[A];
-    const std::vector<int>& cols = tlist[Bt];
-    std::vector<double> qcols(cols.size());
-    for (size_t c = 0; c < cols.size(); ++c) qcols[c] = Q[cols[c]];
-    std::vector<long long> cum_np(cols.size() + 1, 0);
-    for (size_t c = 0; c < cols.size(); ++c) cum_np[c + 1] = cum_np[c] + o->pair_nprim[cols[c]];
+    const std::vector<int>& rows = *tlist[A];
+    const std::vector<int>& cols = *tlist[Bt];
+    const std::vector<double>& qcols = tq[Bt];
     // FP32 recurrences only where they replace real work (total l >= 4) and where the estimated
     // FP32 error of the quartet, kFp32ErrScale * (qp amp)_ab * (qp amp)_cd * c2s amplification,
     // stays below fp32_budget.  qp is the primitive-absolute bound sum_ab q_ab; amp bounds the
@@ -2040,7 +2101,7 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
                        c2s_amp(t.ll, p->sph));
     // suffix maxima of qp*amp over the Q-sorted columns: the FP32 tail of a row starts where
     // (qp amp)_row * (largest qp amp still ahead) < fp32_thr
-    std::vector<double> qp_sufmax(cols.size() + 1, 0.0);
+    std::vector<double> qp_sufmax(fp32_class ? cols.size() + 1 : 0, 0.0);
     if (fp32_class)
       for (size_t c = cols.size(); c-- > 0;)
         qp_sufmax[c] = std::max(qp_sufmax[c + 1], o->pair_qp[cols[c]] * o->pair_amp[cols[c]]);
@@ -2050,11 +2111,14 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
     t32.fp32 = true;
     t.row_prefix.push_back(0);
     t32.row_prefix.push_back(0);
+    // count of cols with qa * Q >= cutoff (cols sorted decreasing): rows come in decreasing Q, so
+    // the count never grows from one row to the next and is found by walking it down
+    long long cq = (long long)qcols.size();
     for (size_t r = 0; r < rows.size(); ++r) {
       const double qa = Q[rows[r]];
-      // count of cols with qa * Q >= cutoff (cols sorted decreasing)
-      long long cnt = std::partition_point(qcols.begin(), qcols.end(), [&](double qb) { return qa * qb >= cutoff; }) -
-                      qcols.begin();
+      while (cq > 0 && !(qa * qcols[cq - 1] >= cutoff)) --cq;
+      if (cq == 0) break;  // and for every later row
+      long long cnt = cq;
       if (A == Bt) cnt = std::min<long long>(cnt, (long long)r + 1);
       if (cnt <= 0) continue;
       long long c64 = cnt;
@@ -2078,8 +2142,9 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
                            nsph_or_cart(t.lk, p->sph) * nsph_or_cart(t.ll, p->sph);
     for (Tile* tp : {&t, &t32}) {
       if (tp->rows.empty()) continue;
-      tp->cols = cols;
-      tp->cum_np = cum_np;
+      tp->cols = tlist[Bt];
+      tp->cum_np = tcum[Bt];
+      tp->nprimq = tile_prim_quartets(*tp, o);
       const long long nq = tp->row_prefix.back();
       R.nq += nq;
       R.nint += nq * nout;
@@ -2108,7 +2173,11 @@ static int build_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, int sp
     nq_fp32 += R.nq32;
     for (Tile& t : R.tiles) p->tiles.push_back(std::move(t));
   }
-  plog.mark("tiles (host)");
+  {
+    char msg[96];
+    snprintf(msg, sizeof msg, "tiles (host; %d pair types, %zu tiles)", nt, p->tiles.size());
+    plog.mark(msg);
+  }
   const int rcf = finish_screened(p, o, ecut, max_chunk, prim_budget, nq_total, nint_total, nq_fp32, plan);
   plog.mark("chunks, segments, device tables");
   return rcf;
@@ -2201,14 +2270,24 @@ int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, 
   p->family = CINTX_INT3C2E;
   p->sph = sph != 0;
   long long nq_total = 0, nint_total = 0;
+  // column types sorted once, shared by their tiles
+  std::vector<std::pair<int, std::shared_ptr<const std::vector<int>>>> ccols;
+  std::vector<std::shared_ptr<const std::vector<long long>>> ccum;
+  for (auto& ck : ctypes) {
+    std::vector<int> cols = ck.second;
+    std::stable_sort(cols.begin(), cols.end(), by_q);
+    std::vector<long long> cum(cols.size() + 1, 0);
+    for (size_t c = 0; c < cols.size(); ++c) cum[c + 1] = cum[c] + o->pair_nprim[cols[c]];
+    ccols.emplace_back(ck.first.first, std::make_shared<const std::vector<int>>(std::move(cols)));
+    ccum.push_back(std::make_shared<const std::vector<long long>>(std::move(cum)));
+  }
   for (auto& rk : rtypes) {
     std::vector<int> rows = rk.second;
     std::stable_sort(rows.begin(), rows.end(), by_q);
     const int la = std::get<0>(rk.first), lb = std::get<1>(rk.first);
-    for (auto& ck : ctypes) {
-      std::vector<int> cols = ck.second;
-      std::stable_sort(cols.begin(), cols.end(), by_q);
-      const int lk = ck.first.first;
+    for (size_t ci = 0; ci < ccols.size(); ++ci) {
+      const std::vector<int>& cols = *ccols[ci].second;
+      const int lk = ccols[ci].first;
       const long long ni = nsph_or_cart(la, p->sph), nj = nsph_or_cart(lb, p->sph), nk = nsph_or_cart(lk, p->sph);
       Tile t;
       t.typeA = t.typeB = 0;
@@ -2234,9 +2313,8 @@ int cintx_plan_int3c2e_screened(CintxPlan** plan, CINTOpt* optp, double cutoff, 
         t.row_prefix.push_back(t.row_prefix.back() + cnt);
       }
       if (t.rows.empty()) continue;
-      t.cols = cols;
-      t.cum_np.assign(cols.size() + 1, 0);
-      for (size_t c = 0; c < cols.size(); ++c) t.cum_np[c + 1] = t.cum_np[c] + o->pair_nprim[cols[c]];
+      t.cols = ccols[ci].second;
+      t.cum_np = ccum[ci];
       nq_total += t.row_prefix.back();
       nint_total += t.row_prefix.back() * ni * nj * nk;
       p->tiles.push_back(t);
