@@ -90,7 +90,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk-doubles", type=int, default=1 << 30,
                     help="largest chunk of the device sweep (output doubles); with N > 1 ranks chunks shrink "
-                         "so that every rank gets about four")
+                         "so that every rank gets about sixteen")
     ap.add_argument("--branches", type=int, default=4)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--form", default="tuned", choices=["tuned", "plain"])
@@ -887,7 +887,7 @@ def our_arm(args):
 
     plan = make_plan(opt, "tuned" if tuned else "plain", args.chunk_doubles)
     cd = chunk_doubles_for(plan.stats.nintegrals, world, args.chunk_doubles)
-    if cd != args.chunk_doubles:  # N > 1: about four chunks per rank for the longest-first split
+    if cd != args.chunk_doubles:  # N > 1: about sixteen chunks per rank for the longest-first split
         args.chunk_doubles = cd
         plan = make_plan(opt, "tuned" if tuned else "plain", cd)
     st = plan.stats
@@ -1125,7 +1125,7 @@ def df_arm(args):
     opt = cx.Optimizer(mol.atm, mol.bas, mol.env, pair_shells=norb)
     p3, p2 = make(opt)
     cd = chunk_doubles_for(p3.stats.nintegrals, world, args.chunk_doubles)
-    if cd != args.chunk_doubles:  # N > 1: about four chunks per rank for the longest-first split
+    if cd != args.chunk_doubles:  # N > 1: about sixteen chunks per rank for the longest-first split
         args.chunk_doubles = cd
         p3, p2 = make(opt)
     s3, s2 = p3.stats, p2.stats

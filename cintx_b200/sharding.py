@@ -27,10 +27,14 @@ def chunks_of(owner, rank: int):
     return [c for c, r in enumerate(owner) if r == rank]
 
 
-def chunk_doubles_for(nintegrals: int, world: int, cap: int, per_rank: int = 4, floor: int = 1 << 22) -> int:
+def chunk_doubles_for(nintegrals: int, world: int, cap: int, per_rank: int = 16, floor: int = 1 << 22) -> int:
     """Chunk size (output doubles) for a sweep of `nintegrals` split over `world` ranks: `cap` on
-    one rank (fewest launches), else small enough that every rank gets about `per_rank` chunks, so
-    the longest-first assignment has items to balance; never below `floor`."""
+    one rank (fewest launches), else small enough that every rank gets about `per_rank` chunks.
+    A screened plan orders its quartets by kernel class, so a chunk holds one or a few classes and
+    the flop estimate the assignment balances is off by a class-dependent factor (2-3x between
+    the one-lane s/p classes and the f classes); with many chunks per class the longest-first
+    assignment deals each class's chunks out over all ranks, so every rank gets a similar class
+    mix and those factors cancel.  Never below `floor`."""
     if world <= 1 or nintegrals <= 0:
         return cap
     want = -(-int(nintegrals) // (per_rank * world))

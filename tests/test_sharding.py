@@ -72,5 +72,5 @@ def test_chunk_size_per_world():
     for world in (2, 4, 8):
         cd = chunk_doubles_for(nint, world, cap)
         assert cd <= cap
-        assert -(-nint // cd) >= 4 * world  # every rank gets about four chunks to balance
+        assert -(-nint // cd) >= 16 * world  # every rank gets about sixteen chunks to balance
     assert chunk_doubles_for(1000, 8, cap) == 1 << 22  # tiny sweeps keep a floor
