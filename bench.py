@@ -679,7 +679,7 @@ def error_vs_libcint(torch, plan, mol, ring, stream, per_class, seed):
 # summary each figure comes from.
 NCU_TRAFFIC_PER_QUARTET = {
     # (dram__bytes_read.sum + dram__bytes_write.sum) of one captured launch / its quartets
-    "(10|00)": ((82505472 + 68205568) / 4594144, "profiles/eri4c_1000_mol120_spdf.md"),
+    "(10|00)": ((81397504 + 62672384) / 4594144, "profiles/eri4c_1000_mol120_spdf.md"),
 }
 
 
